@@ -1,0 +1,418 @@
+#!/usr/bin/env python
+"""SpMV throughput benchmark (GB/s and % of HBM peak per format).
+
+Workload (default): the power-law matrix n = 4,194,304 (lognormal rows, mean
+16, sigma 1.2, cap 4096; 70 % of entries within +-1024 of the diagonal, 30 %
+uniform; values U[-1,1]; seed 1), nnz ~ 67.1 M, synthetic.
+
+One step = one y = A x pass (alpha 1, beta 0) for every (format, precision)
+case below, one after another on one stream.  ``value`` = algorithmic bytes of
+all cases / device time of the step (GB/s, whole job over all ranks).  The
+algorithmic bytes of a case are the format's own arrays read once, x read
+once and y written once (no re-reads counted).  The matrix (>= 0.5 GB per
+case) is larger than the 126 MB L2, so every step streams it from HBM; x
+(16-32 MB) is meant to stay L2-resident.
+
+``--impl reference`` times the reference's own scalar/OpenMP code on the host
+(RVVLASparse src/scalar compiled by oracle/Makefile) on the same workload and
+prints the same JSON line.  Under torchrun each rank runs a replica of the
+whole workload (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpMV GB/s & % of HBM peak per format; mixed vs FP64 GPU at <=1e-6 rel err"
+N_DEFAULT = 1 << 22
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def traffic_table() -> dict:
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    return json.load(open(p)) if os.path.exists(p) else {}
+
+
+def workload(name: str, n: int):
+    from rvvlasparse_b200 import workloads as W
+
+    if name == "powerlaw":
+        return W.powerlaw(n, seed=1)
+    if name == "stencil":
+        return W.stencil27(128, seed=3)
+    if name == "laplace":
+        return W.laplace2d(256)
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ----------------------------------------------------------------- GPU cases
+class Case:
+    """One (format, precision) SpMV on the device."""
+
+    def __init__(self, name, mat, prec, nbytes, nnz, m, n):
+        import torch
+
+        self.name, self.mat, self.prec, self.bytes, self.nnz = name, mat, prec, nbytes, nnz
+        vt = torch.float64 if prec == "f64" else torch.float32
+        self.vt = vt
+        self.x = torch.empty(n, dtype=vt, device="cuda")
+        self.y = torch.zeros(m, dtype=vt, device="cuda")
+        self.kernel_ms = []
+
+    def launch(self):
+        import rvvlasparse_b200 as R
+
+        fn = R.sparse_mv_mixed if self.prec.startswith("mixed") else R.sparse_mv
+        st = fn(R.SPARSE_OPERATION_NON_TRANSPOSE, 1.0, self.mat, R.sparse_matrix_descr(), self.x, 0.0, self.y)
+        if st.code != 0:
+            raise RuntimeError(f"{self.name}: status {st.code}: {R.load().rvvla_last_error().decode()}")
+
+
+def crs_bytes(m, n, nnz, vb, xb):
+    return nnz * (vb + 4) + (m + 1) * 4 + n * xb + m * xb
+
+
+def hcsr_bytes(H, vb, xb):
+    nb1 = H.b_m * H.b_n + 1
+    return H.nz * (vb + 2) + H.row_ptr.numel() * 4 + nb1 * 8 + H.n * xb + H.m * xb
+
+
+def build_cases(m, n, Rst, Col, Val, formats, precs):
+    import torch
+
+    import rvvlasparse_b200 as R
+
+    cases = []
+    A64 = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
+    A32 = A64.astype(torch.float32)
+    nnz = A64.nz
+    x64 = torch.as_tensor(np.random.default_rng(0).uniform(-1, 1, n)).cuda()
+    for fmt in formats:
+        if fmt == "crs":
+            for p in precs:
+                if p == "f64":
+                    cases.append(Case("crs_f64", A64, "f64", crs_bytes(m, n, nnz, 8, 8), nnz, m, n))
+                elif p == "f32":
+                    cases.append(Case("crs_f32", A32, "f32", crs_bytes(m, n, nnz, 4, 4), nnz, m, n))
+                elif p == "mixed":
+                    cases.append(Case("crs_mixed", A32, "mixed", crs_bytes(m, n, nnz, 4, 4), nnz, m, n))
+        elif fmt == "hcsr":
+            H64 = R.spMtxHCSR()
+            R.convert(H64, A64, R.convertParams())
+            H32 = R.spMtxHCSR()
+            R.convert(H32, A32, R.convertParams())
+            for p in precs:
+                if p == "f64":
+                    cases.append(Case("hcsr_f64", H64, "f64", hcsr_bytes(H64, 8, 8), nnz, m, n))
+                elif p == "f32":
+                    cases.append(Case("hcsr_f32", H32, "f32", hcsr_bytes(H32, 4, 4), nnz, m, n))
+                elif p == "mixed":
+                    cases.append(Case("hcsr_mixed", H32, "mixed", hcsr_bytes(H32, 4, 4), nnz, m, n))
+    for c in cases:
+        c.x.copy_(x64.to(c.vt))
+    return cases
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during timing."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import rvvlasparse_b200 as R
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lib = R.load()
+    m, n, Rst, Col, Val = workload(args.workload, args.n)
+    cases = build_cases(m, n, Rst, Col, Val, args.formats.split(","), args.precisions.split(","))
+    stream = torch.cuda.current_stream()
+    for _ in range(max(args.warmup, 3)):
+        for c in cases:
+            c.launch()
+    torch.cuda.synchronize()
+
+    # ---- device-timed step (inputs resident in HBM)
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in cases]
+          for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.rvvla_kernel_launch_count()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for s in range(args.steps):
+        for c, (e0, e1) in zip(cases, ev[s]):
+            e0.record(stream)
+            c.launch()
+            e1.record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.rvvla_kernel_launch_count() - l0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    step_ms = t_start.elapsed_time(t_end) / args.steps
+    for s in range(args.steps):
+        for c, (e0, e1) in zip(cases, ev[s]):
+            c.kernel_ms.append(e0.elapsed_time(e1))
+    if world > 1:
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    total_bytes = sum(c.bytes for c in cases)
+    value = total_bytes * world / (step_ms * 1e-3) / 1e9
+
+    # ---- end-to-end through the API with host buffers (H2D x, D2H y inside)
+    e2e_ms, h2d, d2h = e2e_time(cases, args, torch)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = total_bytes * world / (e2e_ms * 1e-3) / 1e9
+
+    pk = peaks()
+    per = {}
+    for c in cases:
+        ms = statistics.median(c.kernel_ms)
+        gbs = c.bytes / (ms * 1e-3) / 1e9
+        per[c.name] = {"ms": round(ms, 4), "gbs": round(gbs, 1), "frac_of_hbm": round(gbs / pk["hbm_gbs"], 4),
+                       "gflops": round(2 * c.nnz / (ms * 1e-3) / 1e9, 1), "bytes": int(c.bytes)}
+    dom = max(cases, key=lambda c: statistics.mean(c.kernel_ms))
+    dom_ms = statistics.mean(dom.kernel_ms)
+    achieved = dom.bytes / (dom_ms * 1e-3) / 1e9
+    tr = traffic_table().get(f"{args.workload}:{dom.name}")
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, m, n, Rst, Col, Val)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": ",".join(sorted({c.prec for c in cases})), "data": "synthetic",
+        "config": {"workload": f"{args.workload} n={m} nnz={len(Col)}", "cases": [c.name for c in cases],
+                   "alpha": 1.0, "beta": 0.0, "parallelism": f"replicas{world}",
+                   "l2": "matrix arrays larger than the 126 MB L2 (streamed from HBM every step); x L2-resident"},
+        "per_format": per,
+        "roofline": {"bound": "hbm", "kernel": dom.name, "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+                     "peak_source": pk["source"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+                     "traffic": tr, "algorithmic_bytes": int(dom.bytes)},
+        "e2e": {"value": round(e2e_value, 1), "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": round(e2e_ms, 4)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def e2e_time(cases, args, torch):
+    """Per step: pinned host x -> device, SpMV, device y -> pinned host."""
+    import rvvlasparse_b200 as R
+
+    stream = torch.cuda.current_stream()
+    hx = [torch.empty(c.x.numel(), dtype=c.vt, pin_memory=True).copy_(c.x.cpu()) for c in cases]
+    hy = [torch.empty(c.y.numel(), dtype=c.vt, pin_memory=True) for c in cases]
+    h2d = sum(h.numel() * h.element_size() for h in hx)
+    d2h = sum(h.numel() * h.element_size() for h in hy)
+
+    def one():
+        for c, x, y in zip(cases, hx, hy):
+            c.x.copy_(x, non_blocking=True)
+            c.launch()
+            y.copy_(c.y, non_blocking=True)
+
+    for _ in range(2):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    _ = R
+    return e0.elapsed_time(e1) / args.steps, h2d, d2h
+
+
+# ----------------------------------------------------------------- CPU side
+def cpu_cases(m, n, Rst, Col, Val, formats, precs):
+    import oracle as O
+
+    out = []
+    for fmt in formats:
+        for p in precs:
+            dt = np.float64 if p == "f64" else np.float32
+            vb, xb = (8, 8) if p == "f64" else (4, 4)
+            A = O.crs(m, n, Rst, Col, Val.astype(dt))
+            if fmt == "crs":
+                out.append((f"crs_{p}", O.ref_crs(A), crs_bytes(m, n, len(Col), vb, xb), dt))
+            elif fmt == "hcsr":
+                h = O.ref_hcsr_convert(A)
+                nb1 = int(h["b_m"]) * int(h["b_n"]) + 1
+                b = len(Col) * (vb + 2) + len(h["row_ptr"]) * 4 + nb1 * 8 + n * xb + m * xb
+                out.append((f"hcsr_{p}", O.ref_hcsr(h), b, dt))
+    return out
+
+
+def cpu_baseline(args, m, n, Rst, Col, Val):
+    """Reference scalar/OpenMP SpMV timed on this host (bounded sample)."""
+    import oracle as O
+
+    if not O.ref_available():
+        return {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "reference library not built"}
+    cases = cpu_cases(m, n, Rst, Col, Val, args.formats.split(","), args.precisions.split(","))
+    x = np.random.default_rng(0).uniform(-1, 1, n)
+    tot_b, tot_t, per = 0, 0.0, {}
+    for name, mat, b, dt in cases:
+        t = mat.time(1.0, x.astype(dt), 0.0, args.cpu_iters)
+        per[name] = round(b / t / 1e9, 2)
+        tot_b += b
+        tot_t += t
+    return {"value": round(tot_b / tot_t / 1e9, 2), "unit": "GB/s", "cores": O.ref_num_threads(),
+            "kind": "reference", "per_format": per,
+            "sample": f"median of {args.cpu_iters} reference sparse_mv calls per case on the full matrix "
+                      f"({', '.join(c[0] for c in cases)}; mixed forms timed as the reference fp32 kernels)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle as O
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference scalar library not built (make -C oracle ref)"}))
+        return
+    m, n, Rst, Col, Val = workload(args.workload, args.n)
+    precs = [p if p != "mixed" else "f32" for p in args.precisions.split(",")]
+    cases = cpu_cases(m, n, Rst, Col, Val, args.formats.split(","), precs)
+    x = np.random.default_rng(0).uniform(-1, 1, n)
+    for _ in range(max(args.warmup, 1)):
+        for name, mat, b, dt in cases:
+            mat.time(1.0, x.astype(dt), 0.0, 1)
+    step_s = []
+    for _ in range(args.steps):
+        s = 0.0
+        for name, mat, b, dt in cases:
+            s += mat.time(1.0, x.astype(dt), 0.0, 1)
+        step_s.append(s)
+    tot_b = sum(c[2] for c in cases)
+    ms = statistics.median(step_s) * 1e3
+    value = tot_b / (ms * 1e-3) / 1e9
+    cores = O.ref_num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": ",".join(sorted(set(precs))), "data": "synthetic",
+        "config": {"workload": f"{args.workload} n={m} nnz={len(Col)}", "cases": [c[0] for c in cases]},
+        "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": cores, "kind": "reference",
+                         "sample": "full matrix, one reference sparse_mv per case per step (OpenMP, all host "
+                                   "threads); mixed forms timed as the reference fp32 kernels"},
+        "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="powerlaw", choices=["powerlaw", "stencil", "laplace"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--formats", default="crs,hcsr")
+    ap.add_argument("--precisions", default="f64,f32,mixed")
+    ap.add_argument("--cpu-iters", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

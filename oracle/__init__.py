@@ -1,0 +1,396 @@
+"""CPU checkers for the SpMV path — TEST INFRASTRUCTURE ONLY.
+
+Two libraries, both built by ``oracle/Makefile``:
+
+* ``_build/liboracle.so`` — our C++ restatement of the reference algorithms
+  (oracle.cpp; each function cites the reference file:line it follows);
+* ``_ref/libref_scalar.so`` — the reference's own scalar sources
+  (RVVLASparse src/scalar/*.cpp) compiled where they lie, behind the
+  ``extern "C"`` shim ref_shim.cpp.  Built only where the reference sources
+  are present; the built file travels with the repository snapshot.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker / the timed CPU
+baseline.  The product (``rvvlasparse_b200``) never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_scalar.so")
+REF_SRC = os.environ.get("RVVLA_REFERENCE_SRC", "/root/reference")
+
+I32, U32, U16, U8, F32, F64, I64, U64 = range(8)
+_NP = {I32: np.int32, U32: np.uint32, U16: np.uint16, U8: np.uint8, F32: np.float32, F64: np.float64,
+       I64: np.int64, U64: np.uint64}
+_CODE = {np.dtype(v): k for k, v in _NP.items()}
+
+_olib = None
+_rlib = None
+
+
+def build(ref: bool = True) -> None:
+    """make -C oracle (and the reference library when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True, capture_output=True)
+    if ref and os.path.isdir(os.path.join(REF_SRC, "src", "scalar")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True, capture_output=True)
+
+
+def _lib():
+    global _olib
+    if _olib is None:
+        if not os.path.exists(ORACLE_LIB):
+            build(ref=False)
+        L = C.CDLL(ORACLE_LIB)
+        vp, i64, dbl, cint = C.c_void_p, C.c_int64, C.c_double, C.c_int
+        sig = {
+            "orc_bundle_new": (vp, [C.c_char_p]), "orc_bundle_free": (None, [vp]),
+            "orc_bundle_fmt": (C.c_char_p, [vp]),
+            "orc_bundle_put": (None, [vp, C.c_char_p, cint, vp, i64]),
+            "orc_bundle_count": (cint, [vp]), "orc_bundle_name": (C.c_char_p, [vp, cint]),
+            "orc_bundle_dtype": (cint, [vp, cint]), "orc_bundle_len": (i64, [vp, cint]),
+            "orc_bundle_data": (vp, [vp, cint]), "orc_bundle_set": (None, [vp, C.c_char_p, dbl]),
+            "orc_bundle_nscalars": (cint, [vp]), "orc_bundle_scalar_name": (C.c_char_p, [vp, cint]),
+            "orc_bundle_scalar": (dbl, [vp, cint]), "orc_last_error": (C.c_char_p, []),
+            "orc_build_hcsr": (vp, [vp, i64, i64, dbl]), "orc_build_sell": (vp, [vp, i64, i64]),
+            "orc_build_csr5": (vp, [vp, i64, i64]), "orc_build_lav": (vp, [vp, i64, dbl, i64]),
+            "orc_build_vnec": (vp, [vp, i64, i64]), "orc_build_vhcc": (vp, [vp, i64, i64]),
+            "orc_build_cvr": (vp, [vp, i64, i64]), "orc_to_crs": (vp, [vp]), "orc_transpose": (vp, [vp]),
+            "orc_spmv": (cint, [vp, dbl, vp, dbl, vp, cint]),
+            "orc_crs_spmv_ld": (None, [vp, dbl, vp, dbl, vp]),
+            "orc_sddmm": (None, [vp, vp, vp, vp]),
+            "orc_merge_path": (None, [i64, vp, i64, i64, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _olib = L
+    return _olib
+
+
+class Bundle:
+    """A format as named numpy arrays + named scalars (``fmt`` tag)."""
+
+    def __init__(self, fmt: str, arrays: dict | None = None, scalars: dict | None = None):
+        self.fmt = fmt
+        self.arrays = dict(arrays or {})
+        self.scalars = dict(scalars or {})
+
+    def __getitem__(self, k):
+        return self.arrays[k] if k in self.arrays else self.scalars[k]
+
+    @property
+    def dtype(self):
+        return np.float32 if int(self.scalars.get("dtype", F64)) == F32 else np.float64
+
+    def _handle(self):
+        L = _lib()
+        h = L.orc_bundle_new(self.fmt.encode())
+        for k, a in self.arrays.items():
+            a = np.ascontiguousarray(a)
+            L.orc_bundle_put(h, k.encode(), _CODE[a.dtype], a.ctypes.data, a.size)
+        for k, v in self.scalars.items():
+            L.orc_bundle_set(h, k.encode(), float(v))
+        return h
+
+    @staticmethod
+    def _from_handle(h) -> "Bundle":
+        L = _lib()
+        b = Bundle(L.orc_bundle_fmt(h).decode())
+        for i in range(L.orc_bundle_count(h)):
+            n, dt, ln = L.orc_bundle_name(h, i).decode(), L.orc_bundle_dtype(h, i), L.orc_bundle_len(h, i)
+            arr = np.empty(ln, dtype=_NP[dt])
+            if ln:
+                C.memmove(arr.ctypes.data, L.orc_bundle_data(h, i), arr.nbytes)
+            b.arrays[n] = arr
+        for i in range(L.orc_bundle_nscalars(h)):
+            b.scalars[L.orc_bundle_scalar_name(h, i).decode()] = L.orc_bundle_scalar(h, i)
+        L.orc_bundle_free(h)
+        return b
+
+
+def crs(m, n, Rst, Col, Val) -> Bundle:
+    Val = np.ascontiguousarray(Val)
+    code = F32 if Val.dtype == np.float32 else F64
+    return Bundle("crs", {"Rst": np.asarray(Rst, np.int32), "Col": np.asarray(Col, np.int32), "Val": Val},
+                  {"m": m, "n": n, "nz": len(Col), "dtype": code})
+
+
+def _run_builder(fn, src: Bundle, *args) -> Bundle:
+    L = _lib()
+    h = src._handle()
+    out = fn(h, *args)
+    L.orc_bundle_free(h)
+    if not out:
+        raise RuntimeError(L.orc_last_error().decode())
+    return Bundle._from_handle(out)
+
+
+def build_hcsr(src, R, C_, p=2.0):
+    return _run_builder(_lib().orc_build_hcsr, src, R, C_, p)
+
+
+def build_sell(src, C_=32, sigma=256):
+    return _run_builder(_lib().orc_build_sell, src, C_, sigma)
+
+
+def build_csr5(src, omega=32, sigma=16):
+    return _run_builder(_lib().orc_build_csr5, src, omega, sigma)
+
+
+def build_lav(src, lanes=8, T=0.2, segment_len=40000):
+    return _run_builder(_lib().orc_build_lav, src, lanes, T, segment_len)
+
+
+def build_vnec(src, nthreads=8, variant=-1):
+    return _run_builder(_lib().orc_build_vnec, src, nthreads, variant)
+
+
+def build_vhcc(src, nthreads=8, vec_size=8):
+    return _run_builder(_lib().orc_build_vhcc, src, nthreads, vec_size)
+
+
+def build_cvr(src, simd_len=8, nthreads=1):
+    return _run_builder(_lib().orc_build_cvr, src, simd_len, nthreads)
+
+
+def to_crs(fmt: Bundle) -> Bundle:
+    return _run_builder(_lib().orc_to_crs, fmt)
+
+
+def transpose(src: Bundle) -> Bundle:
+    return _run_builder(_lib().orc_transpose, src)
+
+
+def spmv(fmt: Bundle, alpha, b, beta, y, stage: int = 3) -> np.ndarray:
+    """Restated reference SpMV; returns the new y (input y is not modified)."""
+    L = _lib()
+    dt = fmt.dtype
+    b = np.ascontiguousarray(b, dtype=dt)
+    out = np.array(y, dtype=dt, copy=True)
+    h = fmt._handle()
+    rc = L.orc_spmv(h, float(alpha), b.ctypes.data, float(beta), out.ctypes.data, stage)
+    L.orc_bundle_free(h)
+    if rc != 0:
+        raise RuntimeError(L.orc_last_error().decode())
+    return out
+
+
+def crs_spmv_ld(src: Bundle, alpha, b, beta, y) -> np.ndarray:
+    """fp64 result of a long-double accumulated CSR SpMV (the FP64 oracle)."""
+    L = _lib()
+    s64 = Bundle("crs", {k: (v.astype(np.float64) if k == "Val" else v) for k, v in src.arrays.items()},
+                 dict(src.scalars, dtype=F64))
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.array(y, dtype=np.float64, copy=True)
+    h = s64._handle()
+    L.orc_crs_spmv_ld(h, float(alpha), b.ctypes.data, float(beta), out.ctypes.data)
+    L.orc_bundle_free(h)
+    return out
+
+
+def sddmm(src: Bundle, g, x) -> np.ndarray:
+    L = _lib()
+    s64 = Bundle("crs", {k: (v.astype(np.float64) if k == "Val" else v) for k, v in src.arrays.items()},
+                 dict(src.scalars, dtype=F64))
+    g = np.ascontiguousarray(g, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.empty(len(src.arrays["Col"]), np.float64)
+    h = s64._handle()
+    L.orc_sddmm(h, g.ctypes.data, x.ctypes.data, out.ctypes.data)
+    L.orc_bundle_free(h)
+    return out
+
+
+def merge_path(diagonal: int, a: np.ndarray, b_len: int):
+    L = _lib()
+    a = np.ascontiguousarray(a, np.int32)
+    out = np.zeros(2, np.int64)
+    L.orc_merge_path(diagonal, a.ctypes.data, len(a), b_len, out.ctypes.data)
+    return int(out[0]), int(out[1])
+
+
+def normwise_relerr(y, yref) -> float:
+    y = np.asarray(y, np.float64)
+    yref = np.asarray(yref, np.float64)
+    den = np.linalg.norm(yref)
+    return float(np.linalg.norm(y - yref) / (den if den > 0 else 1.0))
+
+
+# ------------------------------------------------------------------ reference
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _ref():
+    global _rlib
+    if _rlib is None:
+        if not os.path.exists(REF_LIB):
+            raise RuntimeError("reference scalar library not built (make -C oracle ref)")
+        L = C.CDLL(REF_LIB)
+        vp, i64, dbl, flt, cint = C.c_void_p, C.c_int64, C.c_double, C.c_float, C.c_int
+        L.refx_last_error.restype = C.c_char_p
+        L.refx_num_threads.restype = cint
+        for S, T in (("f64", dbl), ("f32", flt)):
+            def p(name, res, args):
+                f = getattr(L, name.replace("@", S))
+                f.restype, f.argtypes = res, args
+            p("refx_crs_new_@", vp, [i64, i64, i64, vp, vp, vp])
+            p("refx_crs_free_@", None, [vp])
+            p("refx_crs_spmv_@", cint, [vp, T, vp, T, vp])
+            p("refx_crs_time_@", dbl, [vp, T, vp, T, cint])
+            p("refx_hcsr_convert_@", vp, [vp, cint, cint, dbl, cint, cint, cint])
+            p("refx_hcsr_new_@", vp, [vp, vp, vp, vp, vp, vp, vp])
+            p("refx_hcsr_free_@", None, [vp])
+            p("refx_hcsr_info_@", None, [vp, vp, vp])
+            p("refx_hcsr_export_@", None, [vp, vp, vp, vp, vp, vp])
+            p("refx_hcsr_spmv_@", cint, [vp, T, vp, T, vp])
+            p("refx_hcsr_time_@", dbl, [vp, T, vp, T, cint])
+            p("refx_sell_new_@", vp, [vp, vp, vp, vp, vp, vp, vp, vp, i64])
+            p("refx_sell_free_@", None, [vp])
+            p("refx_sell_spmv_@", cint, [vp, cint, T, vp, T, vp])
+            p("refx_sell_time_@", dbl, [vp, T, vp, T, cint])
+            p("refx_lav_new_@", vp, [vp, dbl, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp])
+            p("refx_lav_free_@", None, [vp])
+            p("refx_lav_spmv_@", cint, [vp, T, vp, T, vp])
+            p("refx_lav_time_@", dbl, [vp, T, vp, T, cint])
+            p("refx_cvr_new_@", vp, [vp, vp, vp, vp, vp, vp])
+            p("refx_cvr_free_@", None, [vp])
+            p("refx_cvr_spmv_@", cint, [vp, T, vp, T, vp])
+            p("refx_cvr_time_@", dbl, [vp, T, vp, T, cint])
+        _rlib = L
+    return _rlib
+
+
+def _sfx(dt) -> str:
+    return "f32" if np.dtype(dt) == np.float32 else "f64"
+
+
+def _a(x, dt):
+    return np.ascontiguousarray(x, dtype=dt)
+
+
+class RefMatrix:
+    """A matrix held by the reference library (owning handle)."""
+
+    def __init__(self, kind: str, handle, dt, keep=()):
+        self.kind, self.h, self.dt, self._keep = kind, handle, np.dtype(dt), keep
+
+    def __del__(self):
+        try:
+            getattr(_ref(), f"refx_{self.kind}_free_{_sfx(self.dt)}")(self.h)
+        except Exception:
+            pass
+
+    def spmv(self, alpha, b, beta, y, stage: int | None = None) -> np.ndarray:
+        L = _ref()
+        b = _a(b, self.dt)
+        out = np.array(y, dtype=self.dt, copy=True)
+        if self.kind == "sell":
+            rc = getattr(L, f"refx_sell_spmv_{_sfx(self.dt)}")(self.h, 3 if stage is None else stage, alpha,
+                                                               b.ctypes.data, beta, out.ctypes.data)
+        else:
+            rc = getattr(L, f"refx_{self.kind}_spmv_{_sfx(self.dt)}")(self.h, alpha, b.ctypes.data, beta,
+                                                                     out.ctypes.data)
+        assert rc == 0
+        return out
+
+    def time(self, alpha, b, beta, iters: int) -> float:
+        L = _ref()
+        b = _a(b, self.dt)
+        return getattr(L, f"refx_{self.kind}_time_{_sfx(self.dt)}")(self.h, alpha, b.ctypes.data, beta, iters)
+
+
+def ref_crs(src: Bundle) -> RefMatrix:
+    dt = src.dtype
+    L = _ref()
+    Rst, Col, Val = _a(src["Rst"], np.int32), _a(src["Col"], np.int32), _a(src["Val"], dt)
+    h = getattr(L, f"refx_crs_new_{_sfx(dt)}")(int(src["m"]), int(src["n"]), int(src["nz"]), Rst.ctypes.data,
+                                                Col.ctypes.data, Val.ctypes.data)
+    return RefMatrix("crs", h, dt)
+
+
+def ref_hcsr_convert(src: Bundle, R=None, C_=None, p=None) -> Bundle:
+    """Runs the reference convert<T, spMtxHCSR, false>; returns the HCSR arrays."""
+    L = _ref()
+    dt = src.dtype
+    s = _sfx(dt)
+    crs_m = ref_crs(src)
+    h = getattr(L, f"refx_hcsr_convert_{s}")(crs_m.h, int(R or 0), int(C_ or 0), float(p or 0.0), R is not None,
+                                            C_ is not None, p is not None)
+    if not h:
+        raise RuntimeError(L.refx_last_error().decode())
+    info = np.zeros(7, np.int64)
+    sizes = np.zeros(5, np.int64)
+    getattr(L, f"refx_hcsr_info_{s}")(h, info.ctypes.data, sizes.ctypes.data)
+    arrs = {"block_ptr": np.empty(sizes[0], np.int32), "row_offset": np.empty(sizes[1], np.uint32),
+            "row_ptr": np.empty(sizes[2], np.uint32), "col_idx": np.empty(sizes[3], np.uint16),
+            "values": np.empty(sizes[4], dt)}
+    getattr(L, f"refx_hcsr_export_{s}")(h, *(arrs[k].ctypes.data for k in
+                                            ("block_ptr", "row_offset", "row_ptr", "col_idx", "values")))
+    getattr(L, f"refx_hcsr_free_{s}")(h)
+    sc = dict(zip(("R", "C", "m", "n", "nz", "b_m", "b_n"), (int(v) for v in info)))
+    sc["dtype"] = F32 if dt == np.float32 else F64
+    return Bundle("hcsr", arrs, sc)
+
+
+def ref_hcsr(b: Bundle) -> RefMatrix:
+    L = _ref()
+    dt = b.dtype
+    info = np.array([b[k] for k in ("R", "C", "m", "n", "nz", "b_m", "b_n")], np.int64)
+    arrs = [_a(b["block_ptr"], np.int32), _a(b["row_offset"], np.uint32), _a(b["row_ptr"], np.uint32),
+            _a(b["col_idx"], np.uint16), _a(b["values"], dt)]
+    sizes = np.array([len(a) for a in arrs], np.int64)
+    h = getattr(L, f"refx_hcsr_new_{_sfx(dt)}")(info.ctypes.data, *(a.ctypes.data for a in arrs), sizes.ctypes.data)
+    return RefMatrix("hcsr", h, dt)
+
+
+def ref_sell(b: Bundle) -> RefMatrix:
+    L = _ref()
+    dt = b.dtype
+    ints = np.array([b[k] for k in ("m", "n", "cnt_b", "nz", "C", "Sigma")], np.int64)
+    arrs = [_a(b[k], np.int32) for k in ("vCl", "vCs", "vBs", "vSBs")]
+    col, perm, val = _a(b["vCol"], np.uint32), _a(b["vPerm"], np.uint32), _a(b["vVal"], dt)
+    h = getattr(L, f"refx_sell_new_{_sfx(dt)}")(ints.ctypes.data, *(a.ctypes.data for a in arrs), col.ctypes.data,
+                                                perm.ctypes.data, val.ctypes.data, len(col))
+    return RefMatrix("sell", h, dt, keep=(arrs, col, perm, val))
+
+
+def ref_lav(b: Bundle) -> RefMatrix:
+    L = _ref()
+    dt = b.dtype
+    ints = np.array([b[k] for k in ("SIMD_Lanes", "m", "n", "nz", "segment_count", "chunk_count", "segment_len")]
+                    + [0], np.int64)
+    co, cf = _a(b["chunk_offsets"], np.int32), _a(b["chunk_offsets_full_mask"], np.int32)
+    sp, oo, mk = _a(b["segment_ptr"], np.uint64), _a(b["out_order"], np.uint32), _a(b["mask"], np.uint16)
+    val, ci = _a(b["val"], dt), _a(b["col_id"], np.uint32)
+    sR, sC, sV = _a(b["sp_Rst"], np.int32), _a(b["sp_Col"], np.int32), _a(b["sp_Val"], dt)
+    lens = np.array([len(co), len(cf), len(sp), len(oo), len(mk), len(val), len(sC)], np.int64)
+    h = getattr(L, f"refx_lav_new_{_sfx(dt)}")(ints.ctypes.data, float(b["T"]), lens.ctypes.data, co.ctypes.data,
+                                               cf.ctypes.data, sp.ctypes.data, oo.ctypes.data, mk.ctypes.data,
+                                               val.ctypes.data, ci.ctypes.data, sR.ctypes.data, sC.ctypes.data,
+                                               sV.ctypes.data)
+    return RefMatrix("lav", h, dt)
+
+
+def ref_cvr(b: Bundle) -> RefMatrix:
+    L = _ref()
+    dt = b.dtype
+    ints = np.array([b[k] for k in ("nItems", "numRows", "numCols", "SIMD_LEN", "Nthreads", "Nthreads_avail")],
+                    np.int64)
+    vals, cols = _a(b["vPack_vec_vals"], dt), _a(b["vPack_vec_cols"], np.uint32)
+    rec, wb = _a(b["vPack_vec_record"], np.int32), _a(b["writeback_pos_record"], np.int32)
+    lens = np.array([len(vals), len(rec), len(wb)], np.int64)
+    h = getattr(L, f"refx_cvr_new_{_sfx(dt)}")(ints.ctypes.data, lens.ctypes.data, vals.ctypes.data,
+                                               cols.ctypes.data, rec.ctypes.data, wb.ctypes.data)
+    return RefMatrix("cvr", h, dt)
+
+
+def ref_num_threads() -> int:
+    return int(_ref().refx_num_threads())

@@ -1,0 +1,120 @@
+"""ctypes binding of the C ABI declared in ``include/rvvla.h``.
+
+The shared library is built in-tree (``rvvlasparse_b200/lib/librvvla_b200.so``)
+by ``rvvlasparse_b200.build``.  Loading fails loudly when it is missing: there
+is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "librvvla_b200.so")
+
+RVVLA_OK = 0
+RVVLA_ERR_INVALID_ARG = 1
+RVVLA_ERR_CUDA = 2
+RVVLA_ERR_FORMAT = 3
+RVVLA_ERR_UNSUPPORTED = 4
+RVVLA_ERR_TOO_LARGE = 5
+RVVLA_ERR_TIMEOUT = 6
+RVVLA_ERR_NO_DEVICE = 7
+
+RVVLA_F64 = 0
+RVVLA_F32 = 1
+RVVLA_BF16 = 2
+
+i64 = C.c_int64
+i32 = C.c_int32
+u64 = C.c_uint64
+vp = C.c_void_p
+dbl = C.c_double
+flt = C.c_float
+cint = C.c_int
+
+
+class RvvlaError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+class rvvla_crs(C.Structure):
+    _fields_ = [("m", i64), ("n", i64), ("nz", i64), ("Rst", vp), ("Col", vp), ("Val", vp), ("plan", vp),
+                ("plan_tiles", i64)]
+
+
+class rvvla_hcsr(C.Structure):
+    _fields_ = [("R", i64), ("C", i64), ("m", i64), ("n", i64), ("nz", i64), ("b_m", i64), ("b_n", i64),
+                ("block_ptr", vp), ("row_offset", vp), ("row_ptr", vp), ("col_idx", vp), ("values", vp),
+                ("row_ptr_len", i64)]
+
+
+class rvvla_hcsr_owned(C.Structure):
+    _fields_ = [("h", rvvla_hcsr), ("block_ptr", vp), ("row_offset", vp), ("row_ptr", vp), ("col_idx", vp),
+                ("values", vp)]
+
+
+_lib = None
+
+
+def _proto(lib, name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+
+
+def load():
+    """Load the library (once) and declare every prototype of rvvla.h."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build the CUDA extension first "
+            "(python -m rvvlasparse_b200.build); there is no CPU fallback")
+    lib = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    _proto(lib, "rvvla_version", C.c_char_p)
+    _proto(lib, "rvvla_status_string", C.c_char_p, cint)
+    _proto(lib, "rvvla_last_error", C.c_char_p)
+    _proto(lib, "rvvla_device_info", cint, P(cint), P(cint), P(cint))
+    _proto(lib, "rvvla_kernel_launch_count", u64)
+    _proto(lib, "rvvla_memcpy", cint, vp, vp, C.c_size_t, vp)
+    # CRS
+    _proto(lib, "rvvla_crs_plan_len", i64, i64, i64, cint)
+    _proto(lib, "rvvla_crs_analyze", cint, P(rvvla_crs), cint, vp, vp)
+    _proto(lib, "rvvla_crs_spmv_f64", cint, P(rvvla_crs), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_crs_spmv_f32", cint, P(rvvla_crs), flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_crs_spmv_mixed", cint, P(rvvla_crs), cint, flt, vp, flt, vp, vp)
+    # HCSR
+    _proto(lib, "rvvla_hcsr_build", cint, P(rvvla_crs), cint, i64, i64, dbl, P(rvvla_hcsr_owned), vp)
+    _proto(lib, "rvvla_hcsr_free", None, P(rvvla_hcsr_owned))
+    _proto(lib, "rvvla_hcsr_spmv_f64", cint, P(rvvla_hcsr), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_hcsr_spmv_f32", cint, P(rvvla_hcsr), flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_hcsr_spmv_mixed", cint, P(rvvla_hcsr), cint, flt, vp, flt, vp, vp)
+    # workloads
+    _proto(lib, "rvvla_gen_laplace2d", i64, i64, vp, vp, vp)
+    _proto(lib, "rvvla_gen_stencil27", i64, i64, u64, vp, vp, vp)
+    _proto(lib, "rvvla_gen_powerlaw", i64, i64, dbl, dbl, i64, i64, dbl, u64, vp, vp, vp)
+    _proto(lib, "rvvla_gen_random_rows", i64, i64, i64, cint, dbl, cint, u64, vp, vp, vp)
+    _proto(lib, "rvvla_gen_vector", None, i64, u64, cint, dbl, dbl, vp)
+    _lib = lib
+    return lib
+
+
+def check(status: int, where: str) -> None:
+    if status != RVVLA_OK:
+        lib = load()
+        raise RvvlaError(status, where, lib.rvvla_last_error().decode())
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/rvvla.h (parsed from the header)."""
+    import re
+
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "rvvla.h")
+    text = open(hdr).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rvvla_[a-z0-9_]+)\s*\(", text)))

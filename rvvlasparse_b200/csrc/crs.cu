@@ -1,0 +1,139 @@
+// crs.cu — y = alpha*A*x + beta*y for spMtxCRS (CSR) on sm_100a.
+//
+// Reference: sparse_mv<T, spMtxCRS, false> (src/scalar/spmv_mtx_crs.cpp:22-71)
+// and the RVV version (src/rvv/spmv_mtx_crs.cpp:22-120): one sequential sum
+// per row, y[i] = tmp*alpha + beta*y[i].
+//
+// B200 mapping: merge-path split (Merrill & Garland) of the item stream
+// "row ends + nonzeros" into tiles of 256 threads x IPT items, so every CTA
+// moves the same number of bytes whatever the row-length distribution
+// (lognormal rows up to 4096 long are the design case).  Per tile:
+//   1. coalesced loads of the tile's row ends and (values, columns) with
+//      L2 evict-first, gather of x with L2 evict-last (x stays resident in the
+//      126 MB L2 while the matrix streams past it); products go to shared
+//      memory;
+//   2. each thread walks IPT items of the merge path in shared memory;
+//   3. a block-wide segmented scan (keys = row ids, non-decreasing) hands each
+//      thread the partial sum of its first row from the threads before it;
+//   4. the row that continues into the next tile leaves a (row, value) carry;
+//      a second kernel adds carries in tile order (no float atomics, results
+//      are bitwise reproducible run to run).
+// The same kernels serve VNEC's L variant (merge-path CSR, vnec.cu).
+#include "rvvla_internal.cuh"
+#include "crs_merge.cuh"
+
+namespace rvvla {
+
+__global__ void merge_plan_kernel(int m, int nnz, const int* __restrict__ Rst, int tile_items, int ntiles,
+                                  int* __restrict__ plan) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles) return;
+  const long long items = (long long)m + nnz;
+  const int diag = (int)min((long long)t * tile_items, items);
+  int lo = max(diag - nnz, 0), hi = min(diag, m);
+  while (lo < hi) {
+    const int piv = (lo + hi) >> 1;
+    if (Rst[piv + 1] <= diag - piv - 1) lo = piv + 1;
+    else hi = piv;
+  }
+  plan[2 * t] = lo;
+  plan[2 * t + 1] = diag - lo;
+}
+
+int64_t crs_tiles(int64_t m, int64_t nz, int ipt) {
+  const int64_t tile = (int64_t)kMergeBlock * ipt;
+  return (m + nz + tile - 1) / tile;
+}
+
+int crs_validate(const rvvla_crs* A, const void* x, const void* y) {
+  if (!A) return fail(RVVLA_ERR_INVALID_ARG, "crs: null descriptor");
+  if (A->m < 0 || A->n < 0 || A->nz < 0) return fail(RVVLA_ERR_INVALID_ARG, "crs: negative size");
+  if (A->m + A->nz >= (int64_t)INT32_MAX - 65536) return fail(RVVLA_ERR_TOO_LARGE, "crs: m + nz exceeds int32 merge-path range");
+  if (A->m > 0 && !A->Rst) return fail(RVVLA_ERR_INVALID_ARG, "crs: null Rst");
+  if (A->nz > 0 && (!A->Col || !A->Val)) return fail(RVVLA_ERR_INVALID_ARG, "crs: null Col/Val");
+  if (A->m > 0 && !y) return fail(RVVLA_ERR_INVALID_ARG, "crs: null y");
+  if (A->nz > 0 && !x) return fail(RVVLA_ERR_INVALID_ARG, "crs: null x");
+  return RVVLA_OK;
+}
+
+int crs_plan_launch(int64_t m, int64_t nz, const int32_t* Rst, int ipt, int32_t* plan, cudaStream_t st) {
+  const int64_t nt = crs_tiles(m, nz, ipt);
+  const int threads = 256;
+  const int64_t blocks = (nt + 1 + threads - 1) / threads;
+  merge_plan_kernel<<<(unsigned)blocks, threads, 0, st>>>((int)m, (int)nz, Rst, kMergeBlock * ipt, (int)nt, plan);
+  RVVLA_LAUNCHED("merge_plan_kernel");
+  return RVVLA_OK;
+}
+
+template <class V, class X, class Ac, class P, class CT, int IPT>
+int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStream_t st) {
+  int rc = crs_validate(A, x, y);
+  if (rc) return rc;
+  if (A->m == 0) return RVVLA_OK;
+  const int64_t nt = crs_tiles(A->m, A->nz, IPT);
+  const int32_t* plan = A->plan;
+  if (plan && A->plan_tiles != nt)
+    return fail(RVVLA_ERR_INVALID_ARG, "crs: plan was built for a different size or value type");
+  const size_t plan_bytes = plan ? 0 : (size_t)(2 * (nt + 1)) * sizeof(int32_t);
+  const size_t row_off = (plan_bytes + 255) / 256 * 256;
+  const size_t val_off = row_off + ((size_t)nt * sizeof(int32_t) + 255) / 256 * 256;
+  Scratch sc;
+  RVVLA_CUDA(sc.alloc(val_off + (size_t)nt * sizeof(CT), st));
+  char* base = sc.as<char>();
+  if (!plan) {
+    rc = crs_plan_launch(A->m, A->nz, A->Rst, IPT, (int32_t*)base, st);
+    if (rc) return rc;
+    plan = (const int32_t*)base;
+  }
+  int32_t* crow = (int32_t*)(base + row_off);
+  CT* cval = (CT*)(base + val_off);
+  merge_spmv_kernel<V, X, Ac, P, CT, IPT><<<(unsigned)nt, kMergeBlock, 0, st>>>(
+      (int)A->m, (int)A->nz, A->Rst, A->Col, (const V*)A->Val, x, y, alpha, beta, plan, crow, cval);
+  RVVLA_LAUNCHED("merge_spmv_kernel");
+  merge_fixup_kernel<X, CT><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>((int)nt, (int)A->m, crow, cval, y, alpha);
+  RVVLA_LAUNCHED("merge_fixup_kernel");
+  return RVVLA_OK;
+}
+
+}  // namespace rvvla
+
+using namespace rvvla;
+
+extern "C" {
+
+int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype) {
+  const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
+  return 2 * (crs_tiles(m, nz, ipt) + 1);
+}
+
+int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, void* stream) {
+  if (!A || !plan) return fail(RVVLA_ERR_INVALID_ARG, "crs_analyze: null argument");
+  if (A->m < 0 || A->nz < 0 || (A->m > 0 && !A->Rst)) return fail(RVVLA_ERR_INVALID_ARG, "crs_analyze: bad matrix");
+  if (A->m + A->nz >= (int64_t)INT32_MAX - 65536) return fail(RVVLA_ERR_TOO_LARGE, "crs_analyze: too large");
+  const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
+  if (A->m == 0) return RVVLA_OK;
+  return crs_plan_launch(A->m, A->nz, A->Rst, ipt, plan, as_stream(stream));
+}
+
+int rvvla_crs_spmv_f64(const rvvla_crs* A, double alpha, const double* x, double beta, double* y, void* stream) {
+  return crs_spmv_impl<double, double, double, double, double, MergeCfg<double>::IPT>(A, alpha, x, beta, y,
+                                                                                      as_stream(stream));
+}
+
+int rvvla_crs_spmv_f32(const rvvla_crs* A, float alpha, const float* x, float beta, float* y, void* stream) {
+  return crs_spmv_impl<float, float, float, float, float, MergeCfg<float>::IPT>(A, alpha, x, beta, y,
+                                                                               as_stream(stream));
+}
+
+int rvvla_crs_spmv_mixed(const rvvla_crs* A, int val_type, float alpha, const float* x, float beta, float* y,
+                         void* stream) {
+  if (val_type == RVVLA_F32)
+    return crs_spmv_impl<float, float, CompF32, float, double, MergeCfg<float>::IPT>(A, alpha, x, beta, y,
+                                                                                    as_stream(stream));
+  if (val_type == RVVLA_BF16)
+    return crs_spmv_impl<__nv_bfloat16, float, CompF32, float, double, MergeCfg<float>::IPT>(A, alpha, x, beta, y,
+                                                                                            as_stream(stream));
+  return fail(RVVLA_ERR_INVALID_ARG, "crs_spmv_mixed: val_type must be RVVLA_F32 or RVVLA_BF16");
+}
+
+}  // extern "C"

@@ -1,0 +1,299 @@
+"""Python mirror of RVVLASparse's SpMV API over the C ABI (GPU only).
+
+Names, fields and argument meaning follow the reference:
+
+* ``sparse_mv(op, alpha, mat, descr, b, beta, y, stage=ALL)`` mirrors
+  ``sparse_mv<T, Mtx, simd, stage>`` (include/spmv_mtx.h:21-29) and returns a
+  ``sparse_matrix_status`` whose ``code`` is 0 on success (the C-ABI status
+  otherwise);
+* ``convert(dist, src, params)`` mirrors ``convert<T, MtxDist, simd>``
+  (include/convert.h:30-31) and raises like the reference's HCSR builder
+  (ValueError for std::invalid_argument, OverflowError for std::length_error,
+  RuntimeError for std::logic_error);
+* the ``spMtx*`` classes carry the reference classes' public fields, with the
+  arrays as CUDA tensors.
+
+Vectors ``b`` and ``y`` are CUDA tensors of the matrix's value type (fp32
+for the mixed-precision forms).  Host numpy vectors are accepted too: they are
+copied to the device and ``y`` is copied back (the end-to-end path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from enum import IntEnum
+
+import numpy as np
+import torch
+
+from . import _capi
+from ._capi import check, load
+
+# ------------------------------------------------------------------ types.h
+
+
+class sparse_operation_t(IntEnum):
+    SPARSE_OPERATION_NON_TRANSPOSE = 0
+    SPARSE_OPERATION_TRANSPOSE = 1
+
+
+class sparse_matrix_mv_stage(IntEnum):
+    SPARSE_MATRIX_MV_PREPARATION = 0
+    SPARSE_MATRIX_MV_MULT = 1
+    SPARSE_MATRIX_MV_GET_RESULTS = 2
+    SPARSE_MATRIX_MV_ALL_STAGES = 3
+
+
+SPARSE_OPERATION_NON_TRANSPOSE = sparse_operation_t.SPARSE_OPERATION_NON_TRANSPOSE
+SPARSE_OPERATION_TRANSPOSE = sparse_operation_t.SPARSE_OPERATION_TRANSPOSE
+SPARSE_MATRIX_MV_PREPARATION = sparse_matrix_mv_stage.SPARSE_MATRIX_MV_PREPARATION
+SPARSE_MATRIX_MV_MULT = sparse_matrix_mv_stage.SPARSE_MATRIX_MV_MULT
+SPARSE_MATRIX_MV_GET_RESULTS = sparse_matrix_mv_stage.SPARSE_MATRIX_MV_GET_RESULTS
+SPARSE_MATRIX_MV_ALL_STAGES = sparse_matrix_mv_stage.SPARSE_MATRIX_MV_ALL_STAGES
+
+
+@dataclass
+class sparse_matrix_status:
+    code: int = 0
+
+
+@dataclass
+class sparse_matrix_descr:
+    pass
+
+
+@dataclass
+class convertParams:
+    """``convertParams{std::map<string, convertValue>}`` (include/convert.h:21-28)."""
+    param: dict = field(default_factory=dict)
+
+    def __init__(self, param: dict | None = None, **kw):
+        self.param = dict(param or {})
+        self.param.update(kw)
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    if t is None or t.numel() == 0:
+        return None
+    return t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _dtype_code(t: torch.dtype) -> int:
+    return {torch.float64: _capi.RVVLA_F64, torch.float32: _capi.RVVLA_F32,
+            torch.bfloat16: _capi.RVVLA_BF16}[t]
+
+
+# ------------------------------------------------------------------ CRS
+
+
+class spMtxCRS:
+    """``spMtxCRS<ValT>`` (include/CRS.h:10-20): m, n, nz, Rst[m+1], Col[nz], Val[nz]."""
+
+    def __init__(self, m: int = 0, n: int = 0, nz: int = 0, Rst=None, Col=None, Val=None):
+        self.m, self.n, self.nz = int(m), int(n), int(nz)
+        self.Rst, self.Col, self.Val = Rst, Col, Val
+        self._plans: dict[int, torch.Tensor] = {}
+
+    @classmethod
+    def from_host(cls, m, n, Rst, Col, Val, dtype=torch.float64, device="cuda"):
+        Rst = torch.as_tensor(np.ascontiguousarray(Rst, dtype=np.int32)).to(device)
+        Col = torch.as_tensor(np.ascontiguousarray(Col, dtype=np.int32)).to(device)
+        Val = torch.as_tensor(np.ascontiguousarray(Val)).to(device=device, dtype=dtype)
+        return cls(m, n, int(Col.numel()), Rst, Col, Val)
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.Val.dtype
+
+    def astype(self, dtype: torch.dtype) -> "spMtxCRS":
+        return spMtxCRS(self.m, self.n, self.nz, self.Rst, self.Col, self.Val.to(dtype))
+
+    def desc(self, plan_dtype: int | None = None) -> _capi.rvvla_crs:
+        d = _capi.rvvla_crs(self.m, self.n, self.nz, _ptr(self.Rst), _ptr(self.Col), _ptr(self.Val), None, 0)
+        if plan_dtype is not None and self.m > 0:
+            plan = self.plan(plan_dtype)
+            d.plan = plan.data_ptr()
+            d.plan_tiles = plan.numel() // 2 - 1
+        return d
+
+    def plan(self, dtype_code: int) -> torch.Tensor:
+        """Merge-path tile split (rvvla_crs_analyze), cached per value type."""
+        key = _capi.RVVLA_F64 if dtype_code == _capi.RVVLA_F64 else _capi.RVVLA_F32
+        if key not in self._plans:
+            lib = load()
+            n = lib.rvvla_crs_plan_len(self.m, self.nz, key)
+            plan = torch.empty(int(n), dtype=torch.int32, device=self.Rst.device)
+            d = _capi.rvvla_crs(self.m, self.n, self.nz, _ptr(self.Rst), _ptr(self.Col), _ptr(self.Val), None, 0)
+            check(lib.rvvla_crs_analyze(C.byref(d), key, plan.data_ptr(), _stream()), "rvvla_crs_analyze")
+            self._plans[key] = plan
+        return self._plans[key]
+
+
+# ------------------------------------------------------------------ HCSR
+
+
+class spMtxHCSR:
+    """``spMtxHCSR<ValT>`` (include/HCSR.h:39-53)."""
+
+    def __init__(self):
+        self.R = self.C = self.m = self.n = self.nz = self.b_m = self.b_n = 0
+        self.block_ptr = self.row_offset = self.row_ptr = self.col_idx = self.values = None
+
+    def desc(self) -> _capi.rvvla_hcsr:
+        return _capi.rvvla_hcsr(self.R, self.C, self.m, self.n, self.nz, self.b_m, self.b_n,
+                                _ptr(self.block_ptr), _ptr(self.row_offset), _ptr(self.row_ptr),
+                                _ptr(self.col_idx), _ptr(self.values),
+                                0 if self.row_ptr is None else self.row_ptr.numel())
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.values.dtype
+
+    def astype(self, dtype: torch.dtype) -> "spMtxHCSR":
+        h = spMtxHCSR()
+        h.__dict__.update(self.__dict__)
+        h.values = self.values.to(dtype)
+        return h
+
+    def to_host(self) -> dict:
+        out = {k: getattr(self, k) for k in ("R", "C", "m", "n", "nz", "b_m", "b_n")}
+        for k in ("block_ptr", "row_offset", "row_ptr", "col_idx", "values"):
+            out[k] = getattr(self, k).cpu().numpy()
+        return out
+
+
+def _owned_to_tensor(ptr: int, n: int, dtype: torch.dtype, device) -> torch.Tensor:
+    """Copy a library-owned device array into a torch tensor."""
+    t = torch.empty(max(n, 0), dtype=dtype, device=device)
+    if n > 0:
+        check(load().rvvla_memcpy(t.data_ptr(), ptr, n * t.element_size(), _stream()), "rvvla_memcpy")
+    return t
+
+
+def _hcsr_convert(dist: spMtxHCSR, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    if src.dtype == torch.float64:
+        R, Cc = 2000, 2000  # convert<double, spMtxHCSR, false> defaults (crs_to_hcsr.cpp:140-142)
+    else:
+        R, Cc = 4000, 4000  # convert<float, spMtxHCSR, false> defaults (crs_to_hcsr.cpp:157-159)
+    p = 2.0
+    if "R" in params.param:
+        R = int(params.param["R"])
+    if "C" in params.param:
+        Cc = int(params.param["C"])
+    if "p" in params.param:
+        p = float(params.param["p"])
+    if R <= 0 or Cc <= 0:
+        raise ValueError("crs_to_HCSR: R and C must be positive")
+    owned = _capi.rvvla_hcsr_owned()
+    d = src.desc()
+    st = lib.rvvla_hcsr_build(C.byref(d), src.Val.element_size(), R, Cc, p, C.byref(owned), _stream())
+    if st != 0:
+        msg = lib.rvvla_last_error().decode()
+        if st == _capi.RVVLA_ERR_INVALID_ARG:
+            raise ValueError(msg)
+        if st == _capi.RVVLA_ERR_TOO_LARGE:
+            raise OverflowError(msg)
+        raise RuntimeError(msg)
+    try:
+        h = owned.h
+        dev = src.Val.device
+        dist.R, dist.C, dist.m, dist.n, dist.nz, dist.b_m, dist.b_n = h.R, h.C, h.m, h.n, h.nz, h.b_m, h.b_n
+        nb1 = h.b_m * h.b_n + 1
+        dist.block_ptr = _owned_to_tensor(owned.block_ptr, nb1, torch.int32, dev)
+        dist.row_offset = _owned_to_tensor(owned.row_offset, nb1, torch.int32, dev)
+        dist.row_ptr = _owned_to_tensor(owned.row_ptr, h.row_ptr_len, torch.int32, dev)
+        dist.col_idx = _owned_to_tensor(owned.col_idx, h.nz, torch.int16, dev)
+        dist.values = _owned_to_tensor(owned.values, h.nz, src.Val.dtype, dev)
+    finally:
+        lib.rvvla_hcsr_free(C.byref(owned))
+
+
+# ------------------------------------------------------------------ dispatch
+
+
+def convert(dist, src: spMtxCRS, params: convertParams | None = None):
+    """``convert<T, MtxDist, simd>(dist, src, params)`` run on the GPU."""
+    params = params or convertParams()
+    builders = _builders()
+    for cls, fn in builders.items():
+        if isinstance(dist, cls):
+            fn(dist, src, params)
+            return dist
+    raise TypeError(f"convert: unsupported destination {type(dist).__name__}")
+
+
+def _builders():
+    return {spMtxHCSR: _hcsr_convert}
+
+
+def _call_spmv(mat, alpha, b: torch.Tensor, beta, y: torch.Tensor, mixed: bool) -> int:
+    lib = load()
+    st = _stream()
+    vt = mat.dtype
+    if isinstance(mat, spMtxCRS):
+        if mixed:
+            d = mat.desc(_capi.RVVLA_F32)
+            return lib.rvvla_crs_spmv_mixed(C.byref(d), _dtype_code(vt), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        if vt == torch.float64:
+            d = mat.desc(_capi.RVVLA_F64)
+            return lib.rvvla_crs_spmv_f64(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        d = mat.desc(_capi.RVVLA_F32)
+        return lib.rvvla_crs_spmv_f32(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    if isinstance(mat, spMtxHCSR):
+        d = mat.desc()
+        if mixed:
+            return lib.rvvla_hcsr_spmv_mixed(C.byref(d), _dtype_code(vt), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        if vt == torch.float64:
+            return lib.rvvla_hcsr_spmv_f64(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        return lib.rvvla_hcsr_spmv_f32(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    raise TypeError(f"sparse_mv: unsupported matrix {type(mat).__name__}")
+
+
+def _vec_type(mat, mixed: bool) -> torch.dtype:
+    return torch.float32 if mixed else mat.dtype
+
+
+def _spmv(op, alpha, mat, descr, b, beta, y, mixed: bool, stage=SPARSE_MATRIX_MV_ALL_STAGES):
+    status = sparse_matrix_status()
+    if int(op) != int(SPARSE_OPERATION_NON_TRANSPOSE):
+        status.code = _capi.RVVLA_ERR_UNSUPPORTED
+        return status
+    vt = _vec_type(mat, mixed)
+    host_y = None
+    if isinstance(b, np.ndarray):
+        b = torch.as_tensor(b).to("cuda", dtype=vt)
+    if isinstance(y, np.ndarray):
+        host_y = y
+        y = torch.as_tensor(y).to("cuda", dtype=vt)
+    if b.dtype != vt or y.dtype != vt or not b.is_cuda or not y.is_cuda:
+        status.code = _capi.RVVLA_ERR_INVALID_ARG
+        return status
+    status.code = _call_spmv(mat, alpha, b, beta, y, mixed) if stage == SPARSE_MATRIX_MV_ALL_STAGES \
+        else _call_stage(mat, alpha, b, beta, y, stage)
+    if host_y is not None and status.code == 0:
+        host_y[...] = y.cpu().numpy()
+    return status
+
+
+def _call_stage(mat, alpha, b, beta, y, stage):
+    # Formats other than SELL-C-sigma have no staged form: PREPARATION and
+    # GET_RESULTS are no-ops and MULT is the whole product.
+    if stage == SPARSE_MATRIX_MV_MULT:
+        return _call_spmv(mat, alpha, b, beta, y, False)
+    return 0
+
+
+def sparse_mv(op, alpha, mat, descr, b, beta, y, stage=SPARSE_MATRIX_MV_ALL_STAGES):
+    """y <- alpha*A*b + beta*y on the GPU (``sparse_mv<T, Mtx, simd, stage>``)."""
+    return _spmv(op, alpha, mat, descr, b, beta, y, False, stage)
+
+
+def sparse_mv_mixed(op, alpha, mat, descr, b, beta, y):
+    """Mixed precision form: values fp32/bf16, b and y fp32, compensated fp32
+    row sums, fp64 cross-tile merges (no reference counterpart)."""
+    return _spmv(op, alpha, mat, descr, b, beta, y, True)
