@@ -95,6 +95,13 @@ def hcsr_bytes(H, vb, xb):
     return H.nz * (vb + 2) + H.row_ptr.numel() * 4 + nb1 * 8 + H.n * xb + H.m * xb
 
 
+def csr5_bytes(m, n, nnz, p, omega, tdl, nofs, vb, xb):
+    # values + columns, row pointer (tail rows), tile pointers, descriptors,
+    # empty-offset pointers/map, x and y
+    return (nnz * (vb + 4) + (m + 1) * 4 + (p + 1) * 4 + max(p - 1, 0) * omega * tdl * 4 + p * 4 + nofs * 4
+            + n * xb + m * xb)
+
+
 def build_cases(m, n, Rst, Col, Val, formats, precs):
     import torch
 
@@ -126,6 +133,15 @@ def build_cases(m, n, Rst, Col, Val, formats, precs):
                     cases.append(Case("hcsr_f32", H32, "f32", hcsr_bytes(H32, 4, 4), nnz, m, n))
                 elif p == "mixed":
                     cases.append(Case("hcsr_mixed", H32, "mixed", hcsr_bytes(H32, 4, 4), nnz, m, n))
+        elif fmt == "csr5":
+            sig = {"f64": 16, "f32": 16, "mixed": 16}
+            for p in precs:
+                src = A64 if p == "f64" else A32
+                C5 = R.spMtxCSR5()
+                R.convert(C5, src, R.convertParams(omega=32, sigma=sig[p]))
+                vb = 8 if p == "f64" else 4
+                b = csr5_bytes(m, n, nnz, C5.p, C5.omega, C5.tile_desc_len, C5.num_offsets, vb, vb)
+                cases.append(Case(f"csr5_{p}", C5, p, b, nnz, m, n))
     for c in cases:
         c.x.copy_(x64.to(c.vt))
     return cases
@@ -332,6 +348,13 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
                 nb1 = int(h["b_m"]) * int(h["b_n"]) + 1
                 b = len(Col) * (vb + 2) + len(h["row_ptr"]) * 4 + nb1 * 8 + n * xb + m * xb
                 out.append((f"hcsr_{p}", O.ref_hcsr(h), b, dt))
+            elif fmt == "csr5":
+                # the reference has CSR5 only as RVV intrinsics: time the
+                # oracle's single-threaded restatement of that kernel
+                c5 = O.build_csr5(A, 32, 16)
+                b = csr5_bytes(m, n, len(Col), int(c5["p"]), 32, int(c5["tile_desc_len"]), int(c5["num_offsets"]),
+                               vb, xb)
+                out.append((f"csr5_{p}", O.OracleMatrix(c5), b, dt))
     return out
 
 
@@ -403,7 +426,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="powerlaw", choices=["powerlaw", "stencil", "laplace"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
-    ap.add_argument("--formats", default="crs,hcsr")
+    ap.add_argument("--formats", default="crs,hcsr,csr5")
     ap.add_argument("--precisions", default="f64,f32,mixed")
     ap.add_argument("--cpu-iters", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -79,9 +79,9 @@ int rvvla_memcpy(void* dst, const void* src, size_t bytes, void* stream);
 
 /* ------------------------------------------------------------ CRS (CSR)
  * spMtxCRS<T> (include/CRS.h:10-20 of the reference): m, n, nz, Rst[m+1],
- * Col[nz], Val[nz].  `plan`/`plan_tiles` are optional: the merge-path tile
- * split produced by rvvla_crs_analyze (2*(plan_tiles+1) int32 entries).  With
- * plan == NULL the SpMV computes it itself every call. */
+ * Col[nz], Val[nz].  `plan`, `plan_tiles`, `plan_kind` are optional (NULL /
+ * 0 / 0): the analysis written by rvvla_crs_analyze.  Without a plan every
+ * call computes a merge-path split itself. */
 typedef struct rvvla_crs {
   int64_t m, n, nz;
   const int32_t* Rst;
@@ -89,13 +89,18 @@ typedef struct rvvla_crs {
   const void* Val;
   const int32_t* plan;
   int64_t plan_tiles;
+  int32_t plan_kind; /* 0: merge-path tiles, 1: warp stream (no empty rows) */
 } rvvla_crs;
 
-/* Size in int32 entries of the plan for rvvla_crs_analyze (value type given
- * because tile size depends on it: RVVLA_F64 or RVVLA_F32; mixed uses F32). */
+/* Size in int32 entries of the plan buffer for rvvla_crs_analyze (the tile
+ * size depends on the value type: RVVLA_F64 or RVVLA_F32; mixed uses F32). */
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype);
-/* Writes the merge-path split of (row ends, nonzeros) into plan[0..len). */
-int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, void* stream);
+/* Analyses the row structure once (synchronises `stream`): matrices without
+ * empty rows get the warp-stream split (kind 1: first row of each 2048-
+ * nonzero warp range), others the merge-path split of (row ends, nonzeros)
+ * (kind 0).  Writes plan[], *plan_tiles and *plan_kind for the descriptor. */
+int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* plan_tiles,
+                      int32_t* plan_kind, void* stream);
 
 /* sparse_mv<double, spMtxCRS, *> — src/scalar/spmv_mtx_crs.cpp:22-46 */
 int rvvla_crs_spmv_f64(const rvvla_crs* A, double alpha, const double* x, double beta, double* y,
@@ -156,6 +161,58 @@ int rvvla_hcsr_spmv_f32(const rvvla_hcsr* A, float alpha, const float* x, float 
  * x, y fp32; per-(row, block) sums in fp32 two-sum, merged across column
  * blocks in fp64. */
 int rvvla_hcsr_spmv_mixed(const rvvla_hcsr* A, int val_type, float alpha, const float* x,
+                          float beta, float* y, void* stream);
+
+/* ------------------------------------------------------------ CSR5
+ * spMtxCSR5<T> (include/CSR5.h:57-88): _m, _n, _nnz, _bit_y_offset,
+ * _bit_seg_offset, _tile_desc_len, _tail_tile_start, _p, _omega, _sigma,
+ * _num_offsets and the arrays _csr_row_pointer, _csr_column_index,
+ * _csr_value (full tiles transposed), _csr5_tile_pointer (p+1),
+ * _csr5_tile_descriptor ((p-1)*omega*tile_desc_len),
+ * _csr5_tile_empty_offset_pointer (p), _csr5_tile_empty_offset.
+ * no_empty_rows (not in the reference class): 1 when every row has a
+ * nonzero (set by rvvla_csr5_build); 0 is always safe. */
+typedef struct rvvla_csr5 {
+  int64_t m, n, nnz;
+  int32_t bit_y_offset, bit_seg_offset, tile_desc_len, tail_tile_start;
+  int32_t p, omega, sigma, num_offsets;
+  const int32_t* csr_row_pointer;
+  const uint32_t* csr_column_index;
+  const void* csr_value;
+  const uint32_t* tile_pointer;
+  const uint32_t* tile_descriptor;
+  const uint32_t* tile_empty_offset_pointer;
+  const uint32_t* tile_empty_offset;
+  int32_t no_empty_rows;
+} rvvla_csr5;
+
+typedef struct rvvla_csr5_owned {
+  rvvla_csr5 h;
+  int32_t* csr_row_pointer;
+  uint32_t* csr_column_index;
+  void* csr_value;
+  uint32_t* tile_pointer;
+  uint32_t* tile_descriptor;
+  uint32_t* tile_empty_offset_pointer;
+  uint32_t* tile_empty_offset;
+} rvvla_csr5_owned;
+
+/* spMtxCSR5::inputCSR + asCSR5 (declared at include/CSR5.h:61-65, never
+ * defined in the reference): builds the layout src/rvv/spmv_mtx_csr5.cpp
+ * decodes, on the GPU.  omega <= 32 (the SpMV needs omega == 32), sigma > 0.
+ * Synchronises `stream`. */
+int rvvla_csr5_build(const rvvla_crs* src, int val_bytes, int omega, int sigma,
+                     rvvla_csr5_owned* out, void* stream);
+void rvvla_csr5_free(rvvla_csr5_owned* h);
+/* sparse_mv<double, spMtxCSR5, true> — src/rvv/spmv_mtx_csr5.cpp:498-541 */
+int rvvla_csr5_spmv_f64(const rvvla_csr5* A, double alpha, const double* x, double beta,
+                        double* y, void* stream);
+/* sparse_mv<float, spMtxCSR5, true> — src/rvv/spmv_mtx_csr5.cpp:543-586 */
+int rvvla_csr5_spmv_f32(const rvvla_csr5* A, float alpha, const float* x, float beta, float* y,
+                        void* stream);
+/* Mixed precision (no reference counterpart): values F32/BF16, x, y fp32,
+ * lane sums fp32 two-sum, cross-lane and cross-tile merges fp64. */
+int rvvla_csr5_spmv_mixed(const rvvla_csr5* A, int val_type, float alpha, const float* x,
                           float beta, float* y, void* stream);
 
 /* ------------------------------------------------------------ workloads

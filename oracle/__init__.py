@@ -182,6 +182,36 @@ def spmv(fmt: Bundle, alpha, b, beta, y, stage: int = 3) -> np.ndarray:
     return out
 
 
+class OracleMatrix:
+    """A format held by the oracle library (marshalled once) for timing the
+    CPU port of kernels the reference only has as RVV intrinsics."""
+
+    def __init__(self, fmt: Bundle):
+        self.fmt = fmt
+        self.dt = np.dtype(fmt.dtype)
+        self.h = fmt._handle()
+
+    def __del__(self):
+        try:
+            _lib().orc_bundle_free(self.h)
+        except Exception:
+            pass
+
+    def time(self, alpha, b, beta, iters: int) -> float:
+        import time as _t
+
+        L = _lib()
+        b = np.ascontiguousarray(b, dtype=self.dt)
+        y = np.zeros(int(self.fmt.scalars.get("m", self.fmt.scalars.get("num_rows", 0))), dtype=self.dt)
+        L.orc_spmv(self.h, float(alpha), b.ctypes.data, float(beta), y.ctypes.data, 3)
+        ts = []
+        for _ in range(iters):
+            t0 = _t.perf_counter()
+            L.orc_spmv(self.h, float(alpha), b.ctypes.data, float(beta), y.ctypes.data, 3)
+            ts.append(_t.perf_counter() - t0)
+        return float(np.median(ts))
+
+
 def crs_spmv_ld(src: Bundle, alpha, b, beta, y) -> np.ndarray:
     """fp64 result of a long-double accumulated CSR SpMV (the FP64 oracle)."""
     L = _lib()

@@ -21,6 +21,7 @@ from .formats import (  # noqa: F401
     sparse_mv,
     sparse_mv_mixed,
     spMtxCRS,
+    spMtxCSR5,
     spMtxHCSR,
 )
 

@@ -42,7 +42,21 @@ class RvvlaError(RuntimeError):
 
 class rvvla_crs(C.Structure):
     _fields_ = [("m", i64), ("n", i64), ("nz", i64), ("Rst", vp), ("Col", vp), ("Val", vp), ("plan", vp),
-                ("plan_tiles", i64)]
+                ("plan_tiles", i64), ("plan_kind", i32)]
+
+
+class rvvla_csr5(C.Structure):
+    _fields_ = [("m", i64), ("n", i64), ("nnz", i64), ("bit_y_offset", i32), ("bit_seg_offset", i32),
+                ("tile_desc_len", i32), ("tail_tile_start", i32), ("p", i32), ("omega", i32), ("sigma", i32),
+                ("num_offsets", i32), ("csr_row_pointer", vp), ("csr_column_index", vp), ("csr_value", vp),
+                ("tile_pointer", vp), ("tile_descriptor", vp), ("tile_empty_offset_pointer", vp),
+                ("tile_empty_offset", vp), ("no_empty_rows", i32)]
+
+
+class rvvla_csr5_owned(C.Structure):
+    _fields_ = [("h", rvvla_csr5), ("csr_row_pointer", vp), ("csr_column_index", vp), ("csr_value", vp),
+                ("tile_pointer", vp), ("tile_descriptor", vp), ("tile_empty_offset_pointer", vp),
+                ("tile_empty_offset", vp)]
 
 
 class rvvla_hcsr(C.Structure):
@@ -84,7 +98,7 @@ def load():
     _proto(lib, "rvvla_memcpy", cint, vp, vp, C.c_size_t, vp)
     # CRS
     _proto(lib, "rvvla_crs_plan_len", i64, i64, i64, cint)
-    _proto(lib, "rvvla_crs_analyze", cint, P(rvvla_crs), cint, vp, vp)
+    _proto(lib, "rvvla_crs_analyze", cint, P(rvvla_crs), cint, vp, P(i64), P(i32), vp)
     _proto(lib, "rvvla_crs_spmv_f64", cint, P(rvvla_crs), dbl, vp, dbl, vp, vp)
     _proto(lib, "rvvla_crs_spmv_f32", cint, P(rvvla_crs), flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_crs_spmv_mixed", cint, P(rvvla_crs), cint, flt, vp, flt, vp, vp)
@@ -94,6 +108,12 @@ def load():
     _proto(lib, "rvvla_hcsr_spmv_f64", cint, P(rvvla_hcsr), dbl, vp, dbl, vp, vp)
     _proto(lib, "rvvla_hcsr_spmv_f32", cint, P(rvvla_hcsr), flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_hcsr_spmv_mixed", cint, P(rvvla_hcsr), cint, flt, vp, flt, vp, vp)
+    # CSR5
+    _proto(lib, "rvvla_csr5_build", cint, P(rvvla_crs), cint, cint, cint, P(rvvla_csr5_owned), vp)
+    _proto(lib, "rvvla_csr5_free", None, P(rvvla_csr5_owned))
+    _proto(lib, "rvvla_csr5_spmv_f64", cint, P(rvvla_csr5), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_csr5_spmv_f32", cint, P(rvvla_csr5), flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_csr5_spmv_mixed", cint, P(rvvla_csr5), cint, flt, vp, flt, vp, vp)
     # workloads
     _proto(lib, "rvvla_gen_laplace2d", i64, i64, vp, vp, vp)
     _proto(lib, "rvvla_gen_stencil27", i64, i64, u64, vp, vp, vp)

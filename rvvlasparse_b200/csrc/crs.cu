@@ -19,10 +19,31 @@
 //      a second kernel adds carries in tile order (no float atomics, results
 //      are bitwise reproducible run to run).
 // The same kernels serve VNEC's L variant (merge-path CSR, vnec.cu).
+#include <algorithm>
+
 #include "rvvla_internal.cuh"
 #include "crs_merge.cuh"
+#include "crs_stream.cuh"
 
 namespace rvvla {
+
+constexpr int kStreamE = 2048;  // nonzeros per warp in the stream kernel
+
+__global__ void crs_stream_plan_kernel(int m, int nnz, const int* __restrict__ Rst, int E, int nwarps,
+                                       int* __restrict__ wrow, int* __restrict__ any_empty) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nwarps) {
+    const int e = t * E;  // largest r with Rst[r] <= e
+    int lo = 0, hi = m + 1;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (Rst[mid] <= e) lo = mid;
+      else hi = mid;
+    }
+    wrow[t] = lo;
+  }
+  if (t < m && Rst[t + 1] == Rst[t]) atomicOr(any_empty, 1);
+}
 
 __global__ void merge_plan_kernel(int m, int nnz, const int* __restrict__ Rst, int tile_items, int ntiles,
                                   int* __restrict__ plan) {
@@ -70,6 +91,24 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
   int rc = crs_validate(A, x, y);
   if (rc) return rc;
   if (A->m == 0) return RVVLA_OK;
+  if (A->plan && A->plan_kind == 1) {  // no empty rows: shared-memory-free stream kernel
+    const int64_t nw = A->plan_tiles;
+    if (nw != (A->nz + kStreamE - 1) / kStreamE || A->nz == 0)
+      return fail(RVVLA_ERR_INVALID_ARG, "crs: stream plan was built for a different matrix");
+    Scratch sc;
+    const size_t row_bytes = ((size_t)(2 * nw) * sizeof(int32_t) + 255) / 256 * 256;
+    RVVLA_CUDA(sc.alloc(row_bytes + (size_t)(2 * nw) * sizeof(CT), st));
+    int32_t* crow = sc.as<int32_t>();
+    CT* cval = (CT*)(sc.as<char>() + row_bytes);
+    crs_stream_kernel<V, X, Ac, CT><<<(unsigned)((nw * 32 + 255) / 256), 256, 0, st>>>(
+        (int)A->m, (int)A->nz, kStreamE, (int)nw, A->Rst, A->Col, (const V*)A->Val, x, y, alpha, beta, A->plan, crow,
+        cval);
+    RVVLA_LAUNCHED("crs_stream_kernel");
+    crs_stream_fixup_kernel<X, CT><<<(unsigned)((2 * nw + 255) / 256), 256, 0, st>>>((int)(2 * nw), crow, cval, y,
+                                                                                       alpha, beta);
+    RVVLA_LAUNCHED("crs_stream_fixup_kernel");
+    return RVVLA_OK;
+  }
   const int64_t nt = crs_tiles(A->m, A->nz, IPT);
   const int32_t* plan = A->plan;
   if (plan && A->plan_tiles != nt)
@@ -87,6 +126,7 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
   }
   int32_t* crow = (int32_t*)(base + row_off);
   CT* cval = (CT*)(base + val_off);
+  prefer_shared(merge_spmv_kernel<V, X, Ac, P, CT, IPT>);
   merge_spmv_kernel<V, X, Ac, P, CT, IPT><<<(unsigned)nt, kMergeBlock, 0, st>>>(
       (int)A->m, (int)A->nz, A->Rst, A->Col, (const V*)A->Val, x, y, alpha, beta, plan, crow, cval);
   RVVLA_LAUNCHED("merge_spmv_kernel");
@@ -103,16 +143,40 @@ extern "C" {
 
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype) {
   const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
-  return 2 * (crs_tiles(m, nz, ipt) + 1);
+  return std::max<int64_t>(2 * (crs_tiles(m, nz, ipt) + 1), (nz + kStreamE - 1) / kStreamE);
 }
 
-int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, void* stream) {
-  if (!A || !plan) return fail(RVVLA_ERR_INVALID_ARG, "crs_analyze: null argument");
+int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* plan_tiles, int32_t* plan_kind,
+                      void* stream) {
+  if (!A || !plan || !plan_tiles || !plan_kind) return fail(RVVLA_ERR_INVALID_ARG, "crs_analyze: null argument");
   if (A->m < 0 || A->nz < 0 || (A->m > 0 && !A->Rst)) return fail(RVVLA_ERR_INVALID_ARG, "crs_analyze: bad matrix");
   if (A->m + A->nz >= (int64_t)INT32_MAX - 65536) return fail(RVVLA_ERR_TOO_LARGE, "crs_analyze: too large");
   const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
+  *plan_tiles = 0;
+  *plan_kind = 0;
   if (A->m == 0) return RVVLA_OK;
-  return crs_plan_launch(A->m, A->nz, A->Rst, ipt, plan, as_stream(stream));
+  cudaStream_t st = as_stream(stream);
+  if (A->nz > 0) {
+    const int64_t nw = (A->nz + kStreamE - 1) / kStreamE;
+    Scratch flag;
+    RVVLA_CUDA(flag.alloc(sizeof(int), st));
+    RVVLA_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    const int64_t n = std::max<int64_t>(nw, A->m);
+    crs_stream_plan_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((int)A->m, (int)A->nz, A->Rst, kStreamE,
+                                                                         (int)nw, plan, flag.as<int>());
+    RVVLA_LAUNCHED("crs_stream_plan_kernel");
+    int any_empty = 1;
+    RVVLA_CUDA(cudaMemcpyAsync(&any_empty, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RVVLA_CUDA(cudaStreamSynchronize(st));
+    if (!any_empty) {
+      *plan_tiles = nw;
+      *plan_kind = 1;
+      return RVVLA_OK;
+    }
+  }
+  *plan_tiles = crs_tiles(A->m, A->nz, ipt);
+  *plan_kind = 0;
+  return crs_plan_launch(A->m, A->nz, A->Rst, ipt, plan, st);
 }
 
 int rvvla_crs_spmv_f64(const rvvla_crs* A, double alpha, const double* x, double beta, double* y, void* stream) {

@@ -30,6 +30,14 @@ __device__ __forceinline__ CompF32 acc_shfl_up(CompF32 a, int d) {
   r.c = __shfl_up_sync(0xffffffffu, a.c, d);
   return r;
 }
+__device__ __forceinline__ double acc_bcast(double a, int l) { return __shfl_sync(0xffffffffu, a, l); }
+__device__ __forceinline__ float acc_bcast(float a, int l) { return __shfl_sync(0xffffffffu, a, l); }
+__device__ __forceinline__ CompF32 acc_bcast(CompF32 a, int l) {
+  CompF32 r;
+  r.s = __shfl_sync(0xffffffffu, a.s, l);
+  r.c = __shfl_sync(0xffffffffu, a.c, l);
+  return r;
+}
 __device__ __forceinline__ double acc_out(double a) { return a; }
 __device__ __forceinline__ float acc_out(float a) { return a; }
 __device__ __forceinline__ float acc_out(const CompF32& a) { return a.value(); }
@@ -63,8 +71,9 @@ merge_spmv_kernel(int m, int nnz, const int* __restrict__ Rst, const int* __rest
                   const int* __restrict__ plan, int* __restrict__ carry_row, CT* __restrict__ carry_val) {
   constexpr int TILE = kMergeBlock * IPT;
   constexpr int NW = kMergeBlock / 32;
-  __shared__ int s_rowend[TILE];
-  __shared__ P s_prod[TILE];
+  // rows + nonzeros of a tile add up to TILE, so row ends (int) and products
+  // share one buffer: row ends from the front, products after them.
+  __shared__ __align__(16) unsigned char s_buf[TILE * (sizeof(P) > sizeof(int) ? sizeof(P) : sizeof(int)) + 16];
   __shared__ Ac s_scan[kMergeBlock];
   __shared__ int s_key[kMergeBlock];
   __shared__ int s_wk0[NW], s_wk31[NW];
@@ -74,6 +83,8 @@ merge_spmv_kernel(int m, int nnz, const int* __restrict__ Rst, const int* __rest
   const int lane = tid & 31, warp = tid >> 5;
   const int x0 = plan[2 * t], y0 = plan[2 * t + 1];
   const int nrows = plan[2 * t + 2] - x0, nnzt = plan[2 * t + 3] - y0;
+  int* s_rowend = reinterpret_cast<int*>(s_buf);
+  P* s_prod = reinterpret_cast<P*>(s_buf + (((size_t)nrows * sizeof(int) + sizeof(P) - 1) / sizeof(P)) * sizeof(P));
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
 
   // 1. stage row ends and products

@@ -179,8 +179,26 @@ template <> __device__ __forceinline__ __nv_bfloat16 ldv<__nv_bfloat16>(const __
 __device__ __forceinline__ float to_float(float v) { return v; }
 __device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
 
+// Finds j with pre[j] <= v < pre[j+1] in a non-decreasing shared array of
+// n+1 entries (pre[0] = 0 <= v < pre[n]).
+__device__ __forceinline__ int find_slot(const int* pre, int n, int v) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // V stored value, X vector type, SA shared accumulator type, MIX: compensated
 // fp32 row sums merged into fp64.
+//
+// Work items of a block-row: every CSR block gives ceil(rows/32) items of 32
+// rows (a lane sums one row of the block); all COO nonzeros of the block-row,
+// taken block after block, form one stream cut into items of 32 nonzeros (a
+// lane finds its block by binary search over the COO prefix in shared
+// memory).  Tiny COO blocks therefore share warps instead of idling them.
 template <class V, class X, class SA, bool MIX>
 __global__ void __launch_bounds__(256)
 hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __restrict__ block_ptr,
@@ -189,68 +207,62 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
                  X* __restrict__ y, X alpha, X beta) {
   extern __shared__ __align__(16) unsigned char smem[];
   SA* acc = reinterpret_cast<SA*>(smem);
-  int* itoff = reinterpret_cast<int*>(smem + ((R * sizeof(SA) + 15) / 16) * 16);
-  __shared__ int s_wsum[8];
+  int* csr_pre = reinterpret_cast<int*>(smem + ((R * sizeof(SA) + 15) / 16) * 16);
+  int* coo_pre = csr_pre + (b_n + 1);
+  __shared__ int s_w[2][8];
   const int64_t br = blockIdx.x;
   const int64_t r0 = br * R;
   const int maxr = (int)min(R, m - r0);
   const int64_t blk0 = br * b_n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int li = tid; li < maxr; li += 256) acc[li] = SA(0);
-  // work items per block, then an inclusive scan over b_n entries
   const int row_items = (maxr + 31) >> 5;
-  int carry = 0;
-  if (tid == 0) itoff[0] = 0;
+  int carry_a = 0, carry_b = 0;
+  if (tid == 0) { csr_pre[0] = 0; coo_pre[0] = 0; }
   for (int64_t j0 = 0; j0 < b_n; j0 += 256) {
     const int64_t j = j0 + tid;
-    int it = 0;
+    int a = 0, b = 0;
     if (j < b_n) {
       const uint32_t ro = row_offset[blk0 + j];
       const int nzb = block_ptr[blk0 + j + 1] - block_ptr[blk0 + j];
-      it = ((ro >> 30) == 1) ? row_items : ((nzb + 31) >> 5);
+      if ((ro >> 30) == 1) a = row_items;
+      else b = nzb;
     }
-    int inc = it;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      int o = __shfl_up_sync(0xffffffffu, inc, d);
-      if (lane >= d) inc += o;
+      const int oa = __shfl_up_sync(0xffffffffu, a, d);
+      const int ob = __shfl_up_sync(0xffffffffu, b, d);
+      if (lane >= d) { a += oa; b += ob; }
     }
-    if (lane == 31) s_wsum[warp] = inc;
+    if (lane == 31) { s_w[0][warp] = a; s_w[1][warp] = b; }
     __syncthreads();
-    int wofs = 0, tot = 0;
+    int wa = 0, wb = 0, ta = 0, tb = 0;
     for (int w = 0; w < 8; ++w) {
-      if (w < warp) wofs += s_wsum[w];
-      tot += s_wsum[w];
+      if (w < warp) { wa += s_w[0][w]; wb += s_w[1][w]; }
+      ta += s_w[0][w];
+      tb += s_w[1][w];
     }
-    if (j < b_n) itoff[j + 1] = carry + wofs + inc;
-    carry += tot;
+    if (j < b_n) { csr_pre[j + 1] = carry_a + wa + a; coo_pre[j + 1] = carry_b + wb + b; }
+    carry_a += ta;
+    carry_b += tb;
     __syncthreads();
   }
-  const int total = carry;
+  const int n_csr = carry_a, n_coo = carry_b;
+  const int total = n_csr + ((n_coo + 31) >> 5);
   for (int item = warp; item < total; item += 8) {
-    int lo = 0, hi = (int)b_n;  // find j with itoff[j] <= item < itoff[j+1]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (itoff[mid] <= item) lo = mid;
-      else hi = mid;
-    }
-    const int64_t j = lo;
-    const int part = item - itoff[j];
-    const int64_t blk = blk0 + j;
-    const uint32_t ro = row_offset[blk];
-    const uint32_t off = ro & kKindMask;
-    const int bp = block_ptr[blk];
-    const X* xb = x + j * C;
-    if ((ro >> 30) == 1) {
+    if (item < n_csr) {
+      const int64_t j = find_slot(csr_pre, (int)b_n, item);
+      const int part = item - csr_pre[j];
+      const int64_t blk = blk0 + j;
+      const uint32_t off = row_offset[blk] & kKindMask;
+      const int bp = block_ptr[blk];
+      const X* xb = x + j * C;
       const int li = part * 32 + lane;
       if (li < maxr) {
         const uint32_t qb = row_ptr[off + li], qe = row_ptr[off + li + 1];
         if constexpr (MIX) {
           CompF32 s;
-          for (uint32_t q = qb; q < qe; ++q) {
-            const float p = to_float(ldv(values + bp + q)) * (float)ldx(xb + col_idx[bp + q]);
-            s.add(p);
-          }
+          for (uint32_t q = qb; q < qe; ++q) s.add(to_float(ldv(values + bp + q)) * (float)ldx(xb + col_idx[bp + q]));
           atomicAdd(&acc[li], (SA)((double)s.s + (double)s.c));
         } else {
           SA s = 0;
@@ -259,13 +271,18 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
         }
       }
     } else {
-      const int q = part * 32 + lane;
-      const int nzb = block_ptr[blk + 1] - bp;
-      if (q < nzb) {
-        const uint32_t li = row_ptr[off + q];
+      const int q = ((item - n_csr) << 5) + lane;
+      if (q < n_coo) {
+        const int64_t j = find_slot(coo_pre, (int)b_n, q);
+        const int64_t blk = blk0 + j;
+        const int k = q - coo_pre[j];
+        const uint32_t off = row_offset[blk] & kKindMask;
+        const int e = block_ptr[blk] + k;
+        const uint32_t li = row_ptr[off + k];
+        const X xv = ldx(x + j * C + col_idx[e]);
         SA p;
-        if constexpr (MIX) p = (SA)(to_float(ldv(values + bp + q)) * (float)ldx(xb + col_idx[bp + q]));
-        else p = (SA)ldv(values + bp + q) * (SA)ldx(xb + col_idx[bp + q]);
+        if constexpr (MIX) p = (SA)(to_float(ldv(values + e)) * (float)xv);
+        else p = (SA)ldv(values + e) * (SA)xv;
         atomicAdd(&acc[li], p);
       }
     }
@@ -296,11 +313,12 @@ int hcsr_spmv_impl(const rvvla_hcsr* A, X alpha, const X* x, X beta, X* y, cudaS
   int rc = hcsr_validate(A, x, y);
   if (rc) return rc;
   if (A->m == 0) return RVVLA_OK;
-  const size_t smem = ((size_t)A->R * sizeof(SA) + 15) / 16 * 16 + (size_t)(A->b_n + 1) * sizeof(int);
+  const size_t smem = ((size_t)A->R * sizeof(SA) + 15) / 16 * 16 + (size_t)(2 * (A->b_n + 1)) * sizeof(int);
   if (smem > 220 * 1024)
-    return fail(RVVLA_ERR_UNSUPPORTED, "hcsr: R*sizeof(acc) + 4*(b_n+1) exceeds 220 KB of shared memory");
+    return fail(RVVLA_ERR_UNSUPPORTED, "hcsr: R*sizeof(acc) + 8*(b_n+1) exceeds 220 KB of shared memory");
   auto kern = hcsr_spmv_kernel<V, X, SA, MIX>;
   if (smem > 48 * 1024) RVVLA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  prefer_shared(kern);
   kern<<<(unsigned)A->b_m, 256, smem, st>>>(A->R, A->C, A->m, A->b_n, A->block_ptr, A->row_offset, A->row_ptr,
                                             A->col_idx, (const V*)A->values, x, y, alpha, beta);
   RVVLA_LAUNCHED("hcsr_spmv_kernel");

@@ -36,6 +36,18 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 int sm_count();
 
+// Ask for the largest shared-memory carveout for a kernel whose occupancy is
+// bounded by its shared memory (set once per kernel instantiation).
+template <class K>
+inline void prefer_shared(K kernel) {
+  static std::atomic<bool> done{false};
+  if (!done.load(std::memory_order_relaxed)) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaGetLastError();
+    done.store(true, std::memory_order_relaxed);
+  }
+}
+
 // Stream-ordered temporary buffer (cudaMallocAsync / cudaFreeAsync).
 struct Scratch {
   void* p = nullptr;

@@ -113,23 +113,27 @@ class spMtxCRS:
         return spMtxCRS(self.m, self.n, self.nz, self.Rst, self.Col, self.Val.to(dtype))
 
     def desc(self, plan_dtype: int | None = None) -> _capi.rvvla_crs:
-        d = _capi.rvvla_crs(self.m, self.n, self.nz, _ptr(self.Rst), _ptr(self.Col), _ptr(self.Val), None, 0)
+        d = _capi.rvvla_crs(self.m, self.n, self.nz, _ptr(self.Rst), _ptr(self.Col), _ptr(self.Val), None, 0, 0)
         if plan_dtype is not None and self.m > 0:
-            plan = self.plan(plan_dtype)
+            plan, tiles, kind = self.plan(plan_dtype)
             d.plan = plan.data_ptr()
-            d.plan_tiles = plan.numel() // 2 - 1
+            d.plan_tiles = tiles
+            d.plan_kind = kind
         return d
 
-    def plan(self, dtype_code: int) -> torch.Tensor:
-        """Merge-path tile split (rvvla_crs_analyze), cached per value type."""
+    def plan(self, dtype_code: int):
+        """Row-structure analysis (rvvla_crs_analyze), cached per value type:
+        (plan tensor, plan_tiles, plan_kind)."""
         key = _capi.RVVLA_F64 if dtype_code == _capi.RVVLA_F64 else _capi.RVVLA_F32
         if key not in self._plans:
             lib = load()
             n = lib.rvvla_crs_plan_len(self.m, self.nz, key)
-            plan = torch.empty(int(n), dtype=torch.int32, device=self.Rst.device)
-            d = _capi.rvvla_crs(self.m, self.n, self.nz, _ptr(self.Rst), _ptr(self.Col), _ptr(self.Val), None, 0)
-            check(lib.rvvla_crs_analyze(C.byref(d), key, plan.data_ptr(), _stream()), "rvvla_crs_analyze")
-            self._plans[key] = plan
+            plan = torch.empty(max(int(n), 1), dtype=torch.int32, device=self.Rst.device)
+            d = _capi.rvvla_crs(self.m, self.n, self.nz, _ptr(self.Rst), _ptr(self.Col), _ptr(self.Val), None, 0, 0)
+            tiles, kind = C.c_int64(0), C.c_int32(0)
+            check(lib.rvvla_crs_analyze(C.byref(d), key, plan.data_ptr(), C.byref(tiles), C.byref(kind), _stream()),
+                  "rvvla_crs_analyze")
+            self._plans[key] = (plan, tiles.value, kind.value)
         return self._plans[key]
 
 
@@ -213,6 +217,76 @@ def _hcsr_convert(dist: spMtxHCSR, src: spMtxCRS, params: convertParams) -> None
         lib.rvvla_hcsr_free(C.byref(owned))
 
 
+# ------------------------------------------------------------------ CSR5
+
+
+class spMtxCSR5:
+    """``spMtxCSR5<ValT>`` (include/CSR5.h:57-88): the underscore fields of the
+    reference without the underscore, arrays on the GPU."""
+
+    SCALARS = ("m", "n", "nnz", "bit_y_offset", "bit_seg_offset", "tile_desc_len", "tail_tile_start", "p",
+               "omega", "sigma", "num_offsets", "no_empty_rows")
+    ARRAYS = ("csr_row_pointer", "csr_column_index", "csr_value", "tile_pointer", "tile_descriptor",
+              "tile_empty_offset_pointer", "tile_empty_offset")
+
+    def __init__(self):
+        for k in self.SCALARS:
+            setattr(self, k, 0)
+        for k in self.ARRAYS:
+            setattr(self, k, None)
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.csr_value.dtype
+
+    def astype(self, dtype: torch.dtype) -> "spMtxCSR5":
+        c = spMtxCSR5()
+        c.__dict__.update(self.__dict__)
+        c.csr_value = self.csr_value.to(dtype)
+        return c
+
+    def desc(self) -> _capi.rvvla_csr5:
+        d = _capi.rvvla_csr5()
+        for k in self.SCALARS:
+            setattr(d, k, int(getattr(self, k)))
+        for k in self.ARRAYS:
+            setattr(d, k, _ptr(getattr(self, k)))
+        return d
+
+    def to_host(self) -> dict:
+        out = {k: int(getattr(self, k)) for k in self.SCALARS}
+        for k in self.ARRAYS:
+            out[k] = getattr(self, k).cpu().numpy()
+        return out
+
+
+def _csr5_convert(dist: spMtxCSR5, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    omega = int(params.param.get("omega", 32))
+    sigma = int(params.param.get("sigma", 16))
+    owned = _capi.rvvla_csr5_owned()
+    d = src.desc()
+    st = lib.rvvla_csr5_build(C.byref(d), src.Val.element_size(), omega, sigma, C.byref(owned), _stream())
+    if st != 0:
+        msg = lib.rvvla_last_error().decode()
+        raise (ValueError if st == _capi.RVVLA_ERR_INVALID_ARG else RuntimeError)(msg)
+    try:
+        h = owned.h
+        dev = src.Val.device
+        for k in spMtxCSR5.SCALARS:
+            setattr(dist, k, int(getattr(h, k)))
+        nfull = max(h.p - 1, 0)
+        sizes = {"csr_row_pointer": (h.m + 1, torch.int32), "csr_column_index": (h.nnz, torch.int32),
+                 "csr_value": (h.nnz, src.Val.dtype), "tile_pointer": (h.p + 1, torch.int32),
+                 "tile_descriptor": (nfull * h.omega * h.tile_desc_len, torch.int32),
+                 "tile_empty_offset_pointer": (h.p, torch.int32),
+                 "tile_empty_offset": (h.num_offsets, torch.int32)}
+        for k, (n, dt) in sizes.items():
+            setattr(dist, k, _owned_to_tensor(getattr(owned, k), n, dt, dev))
+    finally:
+        lib.rvvla_csr5_free(C.byref(owned))
+
+
 # ------------------------------------------------------------------ dispatch
 
 
@@ -228,7 +302,7 @@ def convert(dist, src: spMtxCRS, params: convertParams | None = None):
 
 
 def _builders():
-    return {spMtxHCSR: _hcsr_convert}
+    return {spMtxHCSR: _hcsr_convert, spMtxCSR5: _csr5_convert}
 
 
 def _call_spmv(mat, alpha, b: torch.Tensor, beta, y: torch.Tensor, mixed: bool) -> int:
@@ -251,6 +325,13 @@ def _call_spmv(mat, alpha, b: torch.Tensor, beta, y: torch.Tensor, mixed: bool) 
         if vt == torch.float64:
             return lib.rvvla_hcsr_spmv_f64(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
         return lib.rvvla_hcsr_spmv_f32(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    if isinstance(mat, spMtxCSR5):
+        d = mat.desc()
+        if mixed:
+            return lib.rvvla_csr5_spmv_mixed(C.byref(d), _dtype_code(vt), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        if vt == torch.float64:
+            return lib.rvvla_csr5_spmv_f64(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        return lib.rvvla_csr5_spmv_f32(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
     raise TypeError(f"sparse_mv: unsupported matrix {type(mat).__name__}")
 
 

@@ -221,3 +221,32 @@ def test_host_vectors_end_to_end():
     assert st.code == 0
     yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.0, np.zeros(m))
     assert O.normwise_relerr(y, yref) < 1e-12
+
+
+def test_crs_stream_plan_selected_and_edge_rows():
+    # no empty rows -> warp-stream kernel; rows of length 1 (32 heads per
+    # chunk), exactly 32, and one row far longer than a warp range
+    rng = np.random.default_rng(1)
+    m, n = 9000, 40000
+    lens = np.ones(m, np.int64)
+    lens[100:164] = 32
+    lens[5000] = 9000
+    lens[7000:7010] = 2048
+    Rst = np.zeros(m + 1, np.int32)
+    Rst[1:] = np.cumsum(lens)
+    Col = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) for k in lens]).astype(np.int32)
+    Val = rng.uniform(-1, 1, len(Col))
+    A = gpu_crs(m, n, Rst, Col, Val)
+    assert A.plan(0)[2] == 1  # stream kind
+    x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, m)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 0.5, x, 2.0, y0)
+    assert O.normwise_relerr(run(A, 0.5, x, 2.0, y0), yref) < 1e-12
+    A32 = gpu_crs(m, n, Rst, Col, Val.astype(np.float32))
+    y32 = run(A32, 0.5, x.astype(np.float32), 2.0, y0.astype(np.float32))
+    assert O.normwise_relerr(y32, yref) < 1e-5
+
+
+def test_crs_empty_rows_use_merge_plan(g):
+    A = gpu_crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    has_empty = np.any(np.diff(g["Rst"]) == 0)
+    assert A.plan(0)[2] == (0 if has_empty else 1)
