@@ -76,6 +76,12 @@ uint64_t rvvla_kernel_launch_count(void);
  * stream synchronisation; for callers that manage memory themselves (the
  * builders hand back library-allocated arrays). */
 int rvvla_memcpy(void* dst, const void* src, size_t bytes, void* stream);
+/* Synchronises `stream`, then reads and clears the device status word that
+ * kernels with bounded waits (the bulk-copy pipelines) set when a wait
+ * expires.  *code = 0 and RVVLA_OK when no wait expired since the last call;
+ * otherwise *code != 0 and RVVLA_ERR_TIMEOUT (results of that call are
+ * invalid). */
+int rvvla_device_status(int* code, void* stream);
 
 /* ------------------------------------------------------------ CRS (CSR)
  * spMtxCRS<T> (include/CRS.h:10-20 of the reference): m, n, nz, Rst[m+1],

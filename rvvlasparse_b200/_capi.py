@@ -96,6 +96,7 @@ def load():
     _proto(lib, "rvvla_device_info", cint, P(cint), P(cint), P(cint))
     _proto(lib, "rvvla_kernel_launch_count", u64)
     _proto(lib, "rvvla_memcpy", cint, vp, vp, C.c_size_t, vp)
+    _proto(lib, "rvvla_device_status", cint, P(cint), vp)
     # CRS
     _proto(lib, "rvvla_crs_plan_len", i64, i64, i64, cint)
     _proto(lib, "rvvla_crs_analyze", cint, P(rvvla_crs), cint, vp, P(i64), P(i32), vp)

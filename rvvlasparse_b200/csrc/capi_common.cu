@@ -25,6 +25,23 @@ int cuda_fail(cudaError_t e, const char* where) {
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// One int per device that kernels with bounded waits set when a wait expires.
+int* device_status_word() {
+  static std::mutex mu;
+  static std::vector<int*> words;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)words.size() <= dev) words.resize((size_t)dev + 1, nullptr);
+  if (!words[(size_t)dev]) {
+    int* p = nullptr;
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+    if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) return nullptr;
+    words[(size_t)dev] = p;
+  }
+  return words[(size_t)dev];
+}
+
 int sm_count() {
   static std::mutex mu;
   static std::vector<int> cache;
@@ -81,6 +98,18 @@ int rvvla_device_info(int* cc_major, int* cc_minor, int* sms) {
 }
 
 uint64_t rvvla_kernel_launch_count(void) { return rvvla::g_launches.load(); }
+
+int rvvla_device_status(int* code, void* stream) {
+  if (!code) return rvvla::fail(RVVLA_ERR_INVALID_ARG, "rvvla_device_status: null code");
+  *code = 0;
+  int* w = rvvla::device_status_word();
+  if (!w) return rvvla::fail(RVVLA_ERR_CUDA, "rvvla_device_status: no status word");
+  cudaStream_t st = rvvla::as_stream(stream);
+  RVVLA_CUDA(cudaStreamSynchronize(st));
+  RVVLA_CUDA(cudaMemcpy(code, w, sizeof(int), cudaMemcpyDeviceToHost));
+  RVVLA_CUDA(cudaMemset(w, 0, sizeof(int)));
+  return *code ? RVVLA_ERR_TIMEOUT : RVVLA_OK;
+}
 
 int rvvla_memcpy(void* dst, const void* src, size_t bytes, void* stream) {
   if (bytes == 0) return RVVLA_OK;

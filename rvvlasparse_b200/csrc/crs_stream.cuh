@@ -119,17 +119,22 @@ crs_stream_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ Rst
       // the open row's earlier partial joins segment 0
       if (rel == 0) acc_merge(s, acc);
       const int last_valid = min(31, ke - 1 - c0);
-      const bool seg_end = valid && ((int)lane == last_valid || ((heads >> (lane + 1)) & 1u));
+      const bool next_head = ((int)lane < 31) && ((heads >> (lane + 1)) & 1u);
+      const bool seg_end = valid && ((int)lane == last_valid || next_head);
       const int row = r + rel;
-      // a segment that ends before the chunk's last valid lane ends its row
-      if (seg_end && (int)lane < last_valid) {
-        if (rel == 0 && !(heads & 1u) && open_is_first && first_open) {
-          cfirst = acc_carry(s);
-          cfirst_row = row;
-        } else {
-          write_row(y, row, alpha, beta, (X)acc_out(s));
-        }
+      // segment 0 continues the open row; when that row is the warp's first
+      // row and began in an earlier warp, its piece becomes a carry (kept
+      // warp-uniform: lane 0 publishes the carry slots)
+      const bool first_piece_ends = !(heads & 1u) && heads != 0u && (__ffs(heads) - 1) <= last_valid &&
+                                    open_is_first && first_open;
+      if (first_piece_ends) {
+        const CT v0 = acc_carry(acc_bcast(s, __ffs(heads) - 2));
+        cfirst = v0;
+        cfirst_row = r;
       }
+      // a segment that ends before the chunk's last valid lane ends its row
+      if (seg_end && (int)lane < last_valid && !(rel == 0 && first_piece_ends))
+        write_row(y, row, alpha, beta, (X)acc_out(s));
       // the segment at the last valid lane stays open
       const Ac tailv = acc_bcast(s, last_valid);
       const unsigned nh = __popc(heads & ((2u << last_valid) - 1u));

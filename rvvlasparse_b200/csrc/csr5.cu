@@ -24,11 +24,13 @@
 // rows use a third kernel (:337-365).  No float atomics: results are
 // bitwise reproducible.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
 #include "rvvla_internal.cuh"
 #include "scan.cuh"
+#include "tma.cuh"
 
 namespace rvvla {
 namespace {
@@ -210,31 +212,73 @@ __device__ __forceinline__ void write_first(X* y, int64_t r, CT v, X alpha, X be
   y[r] = (beta == X(0)) ? o : o + beta * y[r];
 }
 
-// One warp per contiguous tile range; omega == 32.
-template <class V, class X, class Ac, class CT, int SIGMA>
-__global__ void __launch_bounds__(256)
-csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, int by, int bsg, int tdl, const uint32_t* __restrict__ colidx,
+constexpr int bits_ce(int v) { return v ? 1 + bits_ce(v >> 1) : 0; }
+
+// Shared-memory pipeline geometry of the bulk-copy kernel: per warp, STAGES
+// tiles of values + columns + descriptors (about 12 KB in flight per warp).
+constexpr int kC5Warps = 4;
+template <class V, int SIGMA>
+struct C5Cfg {
+  static constexpr int WS = 32 * SIGMA;
+  static constexpr int TDL = (bits_ce(32 * SIGMA) + 6 + SIGMA + 31) / 32;
+  static constexpr int VAL_B = WS * (int)sizeof(V);
+  static constexpr int COL_B = WS * 4;
+  static constexpr int DESC_B = 128 * TDL;
+  static constexpr int STAGE_B = VAL_B + COL_B + DESC_B;
+  static constexpr int STAGES = (12800 / STAGE_B) > 2 ? (12800 / STAGE_B) : 2;
+  static constexpr int SMEM = kC5Warps * (STAGES * STAGE_B + STAGES * 8);
+};
+
+// One warp per contiguous tile range; omega == 32.  Lane 0 of each warp
+// streams its tiles into a private STAGES-deep shared-memory ring with 1-D
+// bulk copies (values, columns, descriptors; L2 evict-first) and mbarrier
+// transaction counts; the warp gathers x for all SIGMA steps from registers
+// while later tiles are in flight.
+template <class V, class X, class Ac, class CT, int SIGMA, bool TMA>
+__global__ void __launch_bounds__(kC5Warps * 32)
+csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, const uint32_t* __restrict__ colidx,
                  const V* __restrict__ vals, const uint32_t* __restrict__ tile_ptr,
                  const uint32_t* __restrict__ desc, const uint32_t* __restrict__ eo_ptr,
                  const uint32_t* __restrict__ eo, const X* __restrict__ x, X* __restrict__ y, X alpha, X beta,
-                 CT* __restrict__ cal, int* __restrict__ cal_row) {
+                 CT* __restrict__ cal, int* __restrict__ cal_row, int* __restrict__ status) {
   using Ops = LaneOps<V, X, Ac, CT>;
-  const int64_t warp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  using Cfg = C5Cfg<V, SIGMA>;
+  // omega = 32 fixes the descriptor layout: bit_y_offset = bits(32*sigma),
+  // bit_seg_offset = bits(32) = 6, so every flag position is a constant
+  constexpr int S = Cfg::STAGES, TDL = Cfg::TDL;
+  constexpr int BY = bits_ce(32 * SIGMA), BS = 6, FLAG0 = 32 - BY - BS;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int wid = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  unsigned char* wbuf = smem + wid * (S * Cfg::STAGE_B);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kC5Warps * S * Cfg::STAGE_B) + wid * S;
+  const int64_t warp = (int64_t)blockIdx.x * kC5Warps + wid;
   const int64_t t0 = warp * tiles_per_warp;
   if (t0 >= nfull) return;
   const int64_t t1 = min(nfull, t0 + tiles_per_warp);
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
-  const int flag0 = 32 - by - bsg;
-  const int bit0 = 31 - by - bsg;
-  // carry: the row in progress across tile boundaries
+  auto issue = [&](int64_t t, int s) {
+    unsigned char* st = wbuf + s * Cfg::STAGE_B;
+    mbar_expect_tx(&bars[s], (uint32_t)Cfg::STAGE_B);
+    bulk_g2s(st, vals + t * Cfg::WS, Cfg::VAL_B, &bars[s], pf);
+    bulk_g2s(st + Cfg::VAL_B, colidx + t * Cfg::WS, Cfg::COL_B, &bars[s], pf);
+    bulk_g2s(st + Cfg::VAL_B + Cfg::COL_B, desc + t * 32 * TDL, Cfg::DESC_B, &bars[s], pf);
+  };
+  if constexpr (TMA) {
+    if (lane == 0) {
+      for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+      fence_mbar_init();
+    }
+    __syncwarp();
+    if (lane == 0)
+      for (int s = 0; s < S && t0 + s < t1; ++s) issue(t0 + s, s);
+  }
   int64_t crow = -1;
   CT cval = 0;
   bool cfirst = true;  // false: the row started before this warp -> calibrator
   {
-    const uint32_t d0 = __shfl_sync(0xffffffffu, desc[t0 * 32 * tdl + lane], 0);
-    const bool clean = (d0 >> bit0) & 1u;
-    if (!clean) {
+    const uint32_t d0 = __shfl_sync(0xffffffffu, desc[t0 * 32 * TDL + lane], 0);
+    if (!((d0 >> (31 - BY - BS)) & 1u)) {
       crow = tile_ptr[t0] & kNoSign;
       cfirst = false;
     }
@@ -254,44 +298,74 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, int by, int bsg, int tdl, co
     cval = 0;
     cfirst = true;
   };
+  using PT = decltype(Ops::prod(V(), X()));
   for (int64_t t = t0; t < t1; ++t) {
-    const int64_t base = t * (32 * SIGMA);
-    uint32_t c[SIGMA];
-    V v[SIGMA];
+    const int64_t it = t - t0;
+    const int s = (int)(it % S);
+    PT prod[SIGMA];
+    uint32_t dw[TDL];
+    if constexpr (TMA) {
+      if (!mbar_wait(&bars[s], (uint32_t)((it / S) & 1))) {
+        // a copy never completed: record it, drain what is in flight, leave
+        if (lane == 0) {
+          atomicOr(status, RVVLA_DEV_ERR_TIMEOUT);
+          for (int64_t u = t + 1; u < t1 && u < t + S; ++u)
+            mbar_wait(&bars[(u - t0) % S], (uint32_t)(((u - t0) / S) & 1));
+        }
+        __syncwarp();
+        return;
+      }
+      const unsigned char* st = wbuf + s * Cfg::STAGE_B;
+      const V* sv = reinterpret_cast<const V*>(st);
+      const uint32_t* sc = reinterpret_cast<const uint32_t*>(st + Cfg::VAL_B);
+      const uint32_t* sd = reinterpret_cast<const uint32_t*>(st + Cfg::VAL_B + Cfg::COL_B);
+      uint32_t c[SIGMA];
+      V v[SIGMA];
 #pragma unroll
-    for (int i = 0; i < SIGMA; ++i) c[i] = ld_stream(colidx + base + i * 32 + lane, pf);
+      for (int i = 0; i < SIGMA; ++i) c[i] = sc[i * 32 + lane];
 #pragma unroll
-    for (int i = 0; i < SIGMA; ++i) v[i] = ld_stream(vals + base + i * 32 + lane, pf);
-    const uint32_t* dt = desc + t * 32 * tdl;
-    uint32_t dw = dt[lane];
+      for (int i = 0; i < SIGMA; ++i) v[i] = sv[i * 32 + lane];
+#pragma unroll
+      for (int d = 0; d < TDL; ++d) dw[d] = sd[d * 32 + lane];
+      // the warp is done with this stage: refill it with tile t+S
+      __syncwarp();
+      if (lane == 0 && t + S < t1) {
+        fence_proxy_async();
+        issue(t + S, s);
+      }
+#pragma unroll
+      for (int i = 0; i < SIGMA; ++i) prod[i] = Ops::prod(v[i], ld_keep(x + c[i], pl));
+    } else {
+      const int64_t base = t * (int64_t)Cfg::WS;
+      uint32_t c[SIGMA];
+      V v[SIGMA];
+#pragma unroll
+      for (int i = 0; i < SIGMA; ++i) c[i] = ld_stream(colidx + base + i * 32 + lane, pf);
+#pragma unroll
+      for (int i = 0; i < SIGMA; ++i) v[i] = ld_stream(vals + base + i * 32 + lane, pf);
+#pragma unroll
+      for (int d = 0; d < TDL; ++d) dw[d] = ld_stream(desc + t * 32 * TDL + d * 32 + lane, pf);
+#pragma unroll
+      for (int i = 0; i < SIGMA; ++i) prod[i] = Ops::prod(v[i], ld_keep(x + c[i], pl));
+    }
     const uint32_t tp = tile_ptr[t];
     const bool empty = (tp >> 31) & 1u;
     const int64_t first = tp & kNoSign;
     const uint32_t optr = empty ? eo_ptr[t] : 0u;
-    uint32_t yoff = dw >> (32 - by);
-    const uint32_t d0 = dw;
-    uint32_t cur = dw << (by + bsg);
-    bool lb = (cur >> 31) & 1u;
+    uint32_t yoff = dw[0] >> (32 - BY);
+    const uint32_t f0 = dw[0] << (BY + BS);  // step i (< FLAG0) at bit 31-i
+    bool lb = (f0 >> 31) & 1u;
     const bool step0_start = lb;
     if (lane == 0) lb = true;
     const bool start = !lb;
     bool incol = lb && lane != 0;
-    Ac sum, fsum;
-    fsum = Ac();
-    sum = Ac();
-    Ops::add(sum, Ops::prod(v[0], ld_keep(x + c[0], pl)));
-    int ly = 0;
+    Ac sum = Ac(), fsum = Ac();
+    Ops::add(sum, prod[0]);
 #pragma unroll
     for (int i = 1; i < SIGMA; ++i) {
-      const X xv = ld_keep(x + c[i], pl);
-      const int norm_i = i - flag0;
-      if (norm_i >= 0 && (norm_i % 32) == 0) {
-        ly++;
-        cur = dt[ly * 32 + lane];
-      }
-      const int ni = (ly == 0) ? i : (norm_i % 32);
-      const bool b = (cur >> (31 - ni)) & 1u;
-      if (b) {
+      const bool flag = (i < FLAG0) ? ((f0 >> (31 - i)) & 1u)
+                                    : ((dw[(i - FLAG0) / 32 + 1] >> (31 - (i - FLAG0) % 32)) & 1u);
+      if (flag) {
         if (incol) {  // a full row that started in this lane
           const uint32_t k = empty ? eo[optr + yoff] : yoff;
           write_first(y, first + 1 + k, (CT)Ops::fin(sum), alpha, beta);
@@ -302,11 +376,11 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, int by, int bsg, int tdl, co
         sum = Ac();
         incol = true;
       }
-      Ops::add(sum, Ops::prod(v[i], xv));
+      Ops::add(sum, prod[i]);
     }
     // lead: the part of this lane that belongs to the previous lane's row
     const CT lead = start ? (incol ? (CT)Ops::fin(fsum) : (CT)Ops::fin(sum)) : CT(0);
-    const bool has_start = step0_start || incol;  // any row start in this lane
+    const bool has_start = step0_start || incol;
     const unsigned stops = __ballot_sync(0xffffffffu, has_start);
     const unsigned ge = stops & (~0u << lane);
     const int e = ge ? __ffs(ge) - 1 : 31;
@@ -319,12 +393,10 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, int by, int bsg, int tdl, co
     CT Tn = shfl_down_ct(T, 1);
     if (lane == 31) Tn = 0;
     const CT lastv = (CT)Ops::fin(sum) + Tn;
-    // the tile's first row piece (lane 0)
     const bool incol0 = __shfl_sync(0xffffffffu, incol, 0);
     const CT fs0 = __shfl_sync(0xffffffffu, (CT)Ops::fin(fsum), 0);
     const CT add = incol0 ? fs0 : __shfl_sync(0xffffffffu, lastv, 0);
     const unsigned incm = __ballot_sync(0xffffffffu, incol);
-    (void)d0;
     if (crow >= 0 && crow != first) flush();
     if (crow == first) cadd(cval, add);
     else {
@@ -333,8 +405,7 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, int by, int bsg, int tdl, co
       cfirst = true;
     }
     if (incm) {
-      // the tile's first row ends here
-      flush();
+      flush();  // the tile's first row ends in this tile
       const int lstar = 31 - __clz(incm);
       if (incol && lane != lstar) {
         const uint32_t k = empty ? eo[optr + yoff] : yoff;
@@ -526,6 +597,18 @@ __global__ void scale_kernel(int64_t m, X* __restrict__ y, X beta) {
   if (i < m) y[i] = (beta == X(0)) ? X(0) : beta * y[i];
 }
 
+// Staging variant of the templated kernel: direct register loads (default;
+// measured faster on B200: up to 28 resident warps per SM against 16 for the
+// per-warp shared-memory ring) or the bulk-copy pipeline
+// (RVVLA_CSR5_STAGING=tma, a tuning knob read once).
+bool csr5_register_variant() {
+  static const bool regs = [] {
+    const char* e = std::getenv("RVVLA_CSR5_STAGING");
+    return !(e && std::string(e) == "tma");
+  }();
+  return regs;
+}
+
 int csr5_validate(const rvvla_csr5* A, const void* x, const void* y) {
   if (!A) return fail(RVVLA_ERR_INVALID_ARG, "csr5: null descriptor");
   if (A->m < 0 || A->n < 0 || A->nnz < 0 || A->p < 1 || A->sigma <= 0 || A->omega <= 0)
@@ -571,18 +654,30 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
     const uint32_t* eo_ptr = A->tile_empty_offset_pointer;
     const uint32_t* eo = A->tile_empty_offset;
     const V* vals = (const V*)A->csr_value;
-    switch (A->sigma) {
+    int* status = device_status_word();
+    if (!status) return fail(RVVLA_ERR_CUDA, "csr5: no device status word");
+    // bulk copies need 16-byte aligned sources; other layouts take the
+    // register-only kernel
+    const bool aligned = ((uintptr_t)A->csr_value % 16 == 0) && ((uintptr_t)A->csr_column_index % 16 == 0) &&
+                         ((uintptr_t)A->tile_descriptor % 16 == 0);
+    const bool use_regs = csr5_register_variant();
+    switch (aligned ? A->sigma : -1) {
 #define CSR5_CASE(S)                                                                                         \
   case S: {                                                                                                  \
-    auto k_ = csr5_spmv_kernel<V, X, Ac, CT, S>;                                                             \
-    k_<<<blocks, 256, 0, st>>>(nfull, tpw, A->bit_y_offset, A->bit_seg_offset, A->tile_desc_len,             \
-                               A->csr_column_index, vals, A->tile_pointer, A->tile_descriptor, eo_ptr, eo, x,  \
-                               y, alpha, beta_eff, cal, cal_row);                                            \
+    auto k_ = csr5_spmv_kernel<V, X, Ac, CT, S, true>;                                                       \
+    if (use_regs) k_ = csr5_spmv_kernel<V, X, Ac, CT, S, false>;                                             \
+    const int smem_ = use_regs ? 0 : C5Cfg<V, S>::SMEM;                                                      \
+    if (A->tile_desc_len != C5Cfg<V, S>::TDL || A->bit_y_offset != bits_ce(32 * S) || A->bit_seg_offset != 6)  \
+      return fail(RVVLA_ERR_FORMAT, "csr5: descriptor widths do not match omega=32, sigma");                 \
+    if (smem_ > 48 * 1024)                                                                                   \
+      RVVLA_CUDA(cudaFuncSetAttribute(k_, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_));              \
+    const int64_t nw_ = nwarps;                                                                              \
+    k_<<<(unsigned)((nw_ + kC5Warps - 1) / kC5Warps), kC5Warps * 32, smem_, st>>>(                           \
+        nfull, tpw, A->csr_column_index, vals, A->tile_pointer,                                              \
+        A->tile_descriptor, eo_ptr, eo, x, y, alpha, beta_eff, cal, cal_row, status);                        \
     break;                                                                                                   \
   }
-      CSR5_CASE(4)
       CSR5_CASE(8)
-      CSR5_CASE(12)
       CSR5_CASE(16)
       CSR5_CASE(24)
       CSR5_CASE(32)

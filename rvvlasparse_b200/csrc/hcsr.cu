@@ -199,8 +199,11 @@ __device__ __forceinline__ int find_slot(const int* pre, int n, int v) {
 // taken block after block, form one stream cut into items of 32 nonzeros (a
 // lane finds its block by binary search over the COO prefix in shared
 // memory).  Tiny COO blocks therefore share warps instead of idling them.
+constexpr int kHcsrThreads = 512;
+constexpr int kHcsrWarps = kHcsrThreads / 32;
+
 template <class V, class X, class SA, bool MIX>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kHcsrThreads)
 hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __restrict__ block_ptr,
                  const uint32_t* __restrict__ row_offset, const uint32_t* __restrict__ row_ptr,
                  const uint16_t* __restrict__ col_idx, const V* __restrict__ values, const X* __restrict__ x,
@@ -209,17 +212,17 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
   SA* acc = reinterpret_cast<SA*>(smem);
   int* csr_pre = reinterpret_cast<int*>(smem + ((R * sizeof(SA) + 15) / 16) * 16);
   int* coo_pre = csr_pre + (b_n + 1);
-  __shared__ int s_w[2][8];
+  __shared__ int s_w[2][kHcsrWarps];
   const int64_t br = blockIdx.x;
   const int64_t r0 = br * R;
   const int maxr = (int)min(R, m - r0);
   const int64_t blk0 = br * b_n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int li = tid; li < maxr; li += 256) acc[li] = SA(0);
+  for (int li = tid; li < maxr; li += kHcsrThreads) acc[li] = SA(0);
   const int row_items = (maxr + 31) >> 5;
   int carry_a = 0, carry_b = 0;
   if (tid == 0) { csr_pre[0] = 0; coo_pre[0] = 0; }
-  for (int64_t j0 = 0; j0 < b_n; j0 += 256) {
+  for (int64_t j0 = 0; j0 < b_n; j0 += kHcsrThreads) {
     const int64_t j = j0 + tid;
     int a = 0, b = 0;
     if (j < b_n) {
@@ -237,7 +240,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
     if (lane == 31) { s_w[0][warp] = a; s_w[1][warp] = b; }
     __syncthreads();
     int wa = 0, wb = 0, ta = 0, tb = 0;
-    for (int w = 0; w < 8; ++w) {
+    for (int w = 0; w < kHcsrWarps; ++w) {
       if (w < warp) { wa += s_w[0][w]; wb += s_w[1][w]; }
       ta += s_w[0][w];
       tb += s_w[1][w];
@@ -249,7 +252,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
   }
   const int n_csr = carry_a, n_coo = carry_b;
   const int total = n_csr + ((n_coo + 31) >> 5);
-  for (int item = warp; item < total; item += 8) {
+  for (int item = warp; item < total; item += kHcsrWarps) {
     if (item < n_csr) {
       const int64_t j = find_slot(csr_pre, (int)b_n, item);
       const int part = item - csr_pre[j];
@@ -288,7 +291,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
     }
   }
   __syncthreads();
-  for (int li = tid; li < maxr; li += 256) {
+  for (int li = tid; li < maxr; li += kHcsrThreads) {
     const X o = (X)acc[li];
     X* yp = y + r0 + li;
     *yp = (beta == X(0)) ? alpha * o : alpha * o + beta * *yp;
@@ -319,7 +322,7 @@ int hcsr_spmv_impl(const rvvla_hcsr* A, X alpha, const X* x, X beta, X* y, cudaS
   auto kern = hcsr_spmv_kernel<V, X, SA, MIX>;
   if (smem > 48 * 1024) RVVLA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   prefer_shared(kern);
-  kern<<<(unsigned)A->b_m, 256, smem, st>>>(A->R, A->C, A->m, A->b_n, A->block_ptr, A->row_offset, A->row_ptr,
+  kern<<<(unsigned)A->b_m, kHcsrThreads, smem, st>>>(A->R, A->C, A->m, A->b_n, A->block_ptr, A->row_offset, A->row_ptr,
                                             A->col_idx, (const V*)A->values, x, y, alpha, beta);
   RVVLA_LAUNCHED("hcsr_spmv_kernel");
   return RVVLA_OK;

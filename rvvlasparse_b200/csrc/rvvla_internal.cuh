@@ -35,6 +35,8 @@ void count_launch(uint64_t n = 1);
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 int sm_count();
+// Per-device status word set by kernels whose bounded waits expired.
+int* device_status_word();
 
 // Ask for the largest shared-memory carveout for a kernel whose occupancy is
 // bounded by its shared memory (set once per kernel instantiation).
@@ -67,52 +69,54 @@ struct Scratch {
 // ------------------------------------------------------------------ loads
 // Streaming operands (values, indices) are read once: evict-first in L2 and
 // no L1 allocation.  The gathered vector x is re-read across the whole matrix:
-// evict-last keeps it resident in the 126 MB L2.
+// evict-last keeps it resident in the 126 MB L2.  The asm statements are not
+// volatile: they are pure reads of data the kernels never write, so the
+// compiler may hoist and batch them to keep many loads in flight.
 __device__ __forceinline__ uint64_t policy_evict_first() {
   uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
 __device__ __forceinline__ uint64_t policy_evict_last() {
   uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
 
 template <class T> __device__ __forceinline__ T ld_stream(const T* p, uint64_t pol);
 template <> __device__ __forceinline__ double ld_stream<double>(const double* p, uint64_t pol) {
   double v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
   return v;
 }
 template <> __device__ __forceinline__ float ld_stream<float>(const float* p, uint64_t pol) {
   float v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
 template <> __device__ __forceinline__ int ld_stream<int>(const int* p, uint64_t pol) {
   int v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
 template <> __device__ __forceinline__ unsigned ld_stream<unsigned>(const unsigned* p, uint64_t pol) {
   unsigned v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
 template <> __device__ __forceinline__ unsigned short ld_stream<unsigned short>(const unsigned short* p, uint64_t pol) {
   unsigned short v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
   return v;
 }
 template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(const __nv_bfloat16* p, uint64_t pol) {
   unsigned short v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
   return __ushort_as_bfloat16(v);
 }
 __device__ __forceinline__ int4 ld_stream_v4(const int4* p, uint64_t pol) {
   int4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.b32 {%0,%1,%2,%3}, [%4], %5;"
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.b32 {%0,%1,%2,%3}, [%4], %5;"
                : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
                : "l"(p), "l"(pol));
   return v;
@@ -121,12 +125,12 @@ __device__ __forceinline__ int4 ld_stream_v4(const int4* p, uint64_t pol) {
 template <class T> __device__ __forceinline__ T ld_keep(const T* p, uint64_t pol);
 template <> __device__ __forceinline__ double ld_keep<double>(const double* p, uint64_t pol) {
   double v;
-  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
   return v;
 }
 template <> __device__ __forceinline__ float ld_keep<float>(const float* p, uint64_t pol) {
   float v;
-  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
 

@@ -88,6 +88,8 @@ def test_csr5_full_size_powerlaw(dt):
     yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.5, y0)
     assert O.normwise_relerr(y, yref) < tol_for(dt)
     assert np.array_equal(y, run(C5, 1.0, x, 0.5, y0))  # bitwise reproducible
+    code = __import__("ctypes").c_int(-1)
+    assert R.load().rvvla_device_status(__import__("ctypes").byref(code), None) == 0 and code.value == 0
 
 
 def test_csr5_rows_crossing_warps_and_short_rows():
