@@ -102,6 +102,39 @@ def csr5_bytes(m, n, nnz, p, omega, tdl, nofs, vb, xb):
             + n * xb + m * xb)
 
 
+def sell_bytes(S, vb, xb):
+    # values + columns (padded slices), four slice arrays, permutation, x, y
+    return S.len * (vb + 4) + S.cnt_b * 16 + S.m * 4 + S.n * xb + S.m * xb
+
+
+def lav_bytes(Lv, vb, xb):
+    # dense steps (values, columns, masks), out_order, chunk offsets (both),
+    # segment pointers, then the sparse part as CRS (with x and y)
+    L, cc, ns = Lv.SIMD_Lanes, Lv.chunk_count, Lv.segment_count
+    dense = Lv.n_steps * L * (vb + 4) + Lv.n_steps * 2 + ns * cc * L * 4 + (2 * cc + 1) * ns * 4 + (ns + 1) * 8
+    return dense + crs_bytes(Lv.m, Lv.n, Lv.sparse_part.nz, vb, xb)
+
+
+def vnec_bytes(Vn, vb, xb):
+    # the source CRS arrays plus the per-thread merge coordinates
+    return crs_bytes(Vn.m, Vn.n, Vn.nz, vb, xb) + Vn.NUM_THREADS_VNEC * 16
+
+
+def vhcc_bytes(Vh, vb, xb):
+    # vectors (values, columns), end-of-row vector list, scan/write masks,
+    # row list, per-thread info, x, y
+    return (Vh.num_vectors * Vh.vec_size * (vb + 4) + Vh.n_eor * 4 + Vh.scan_mask_bytes + Vh.n_rowarr * 4
+            + Vh.num_threads * 40 + Vh.num_cols * xb + Vh.num_rows * xb)
+
+
+def cvr_bytes(Cv, vb, xb):
+    return Cv.nItems * (vb + 4) + Cv.n_record * 4 + Cv.n_writeback * 4 + Cv.numCols * xb + Cv.numRows * xb
+
+
+# formats whose SpMV has a mixed-precision form
+MIXED = ("crs", "hcsr", "csr5", "sell")
+
+
 def build_cases(m, n, Rst, Col, Val, formats, precs):
     import torch
 
@@ -142,6 +175,25 @@ def build_cases(m, n, Rst, Col, Val, formats, precs):
                 vb = 8 if p == "f64" else 4
                 b = csr5_bytes(m, n, nnz, C5.p, C5.omega, C5.tile_desc_len, C5.num_offsets, vb, vb)
                 cases.append(Case(f"csr5_{p}", C5, p, b, nnz, m, n))
+        elif fmt in ("sell", "lav", "vnec", "vhcc", "cvr"):
+            cls, params, nbytes = {
+                "sell": (R.spMtxSELL_C_Sigma, dict(C=32, sigma=256), sell_bytes),
+                "lav": (R.spMtxLAV, dict(SIMD_Lanes=8, T=0.2, segment_len=40000), lav_bytes),
+                "vnec": (R.spMtxVNEC, {}, vnec_bytes),
+                "vhcc": (R.spMtxVHCC, {}, vhcc_bytes),
+                "cvr": (R.spMtxCVR, {}, cvr_bytes)}[fmt]
+            built = {}
+            for p in precs:
+                if p == "mixed" and fmt not in MIXED:
+                    continue
+                src = A64 if p == "f64" else A32
+                key = "f64" if p == "f64" else "f32"
+                if key not in built:
+                    M = cls()
+                    R.convert(M, src, R.convertParams(**params))
+                    built[key] = M
+                vb = 8 if p == "f64" else 4
+                cases.append(Case(f"{fmt}_{p}", built[key], p, nbytes(built[key], vb, vb), nnz, m, n))
     for c in cases:
         c.x.copy_(x64.to(c.vt))
     return cases
@@ -336,11 +388,18 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
     import oracle as O
 
     out = []
+    crs = {}
     for fmt in formats:
         for p in precs:
+            if p == "mixed" and fmt not in MIXED:
+                continue
+            # the reference has no mixed-precision kernels: its fp32 kernel
+            # stands in for the mixed forms
             dt = np.float64 if p == "f64" else np.float32
             vb, xb = (8, 8) if p == "f64" else (4, 4)
-            A = O.crs(m, n, Rst, Col, Val.astype(dt))
+            if dt not in crs:
+                crs[dt] = O.crs(m, n, Rst, Col, Val.astype(dt))
+            A = crs[dt]
             if fmt == "crs":
                 out.append((f"crs_{p}", O.ref_crs(A), crs_bytes(m, n, len(Col), vb, xb), dt))
             elif fmt == "hcsr":
@@ -355,6 +414,32 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
                 b = csr5_bytes(m, n, len(Col), int(c5["p"]), 32, int(c5["tile_desc_len"]), int(c5["num_offsets"]),
                                vb, xb)
                 out.append((f"csr5_{p}", O.OracleMatrix(c5), b, dt))
+            elif fmt == "sell":
+                sb = O.build_sell(A, 32, 256)
+                b = int(sb["len"]) * (vb + 4) + int(sb["cnt_b"]) * 16 + m * 4 + n * xb + m * xb
+                out.append((f"sell_{p}", O.ref_sell(sb), b, dt))
+            elif fmt == "lav":
+                lb = O.build_lav(A, 8, 0.2, 40000)
+                L, cc, ns, st = 8, int(lb["chunk_count"]), int(lb["segment_count"]), len(lb["mask"])
+                b = (st * L * (vb + 4) + st * 2 + ns * cc * L * 4 + (2 * cc + 1) * ns * 4 + (ns + 1) * 8
+                     + crs_bytes(m, n, int(lb["sparse_nz"]), vb, xb))
+                out.append((f"lav_{p}", O.ref_lav(lb), b, dt))
+            elif fmt == "cvr":
+                # the reference kernel runs one OpenMP thread per CVR thread block
+                cb = O.build_cvr(A, 8, O.ref_num_threads())
+                b = len(cb["vPack_vec_vals"]) * (vb + 4) + len(cb["vPack_vec_record"]) * 4 \
+                    + len(cb["writeback_pos_record"]) * 4 + n * xb + m * xb
+                out.append((f"cvr_{p}", O.ref_cvr(cb), b, dt))
+            elif fmt in ("vnec", "vhcc"):
+                # RVV-only in the reference: the oracle's single-threaded port
+                if fmt == "vnec":
+                    ob = O.build_vnec(A, 16, -1)
+                    b = crs_bytes(m, n, len(Col), vb, xb) + 16 * 16
+                else:
+                    ob = O.build_vhcc(A, 16, 8)
+                    b = (len(ob["vals_arr"]) * (vb + 4) + len(ob["veceor_ptr"]) * 4 + len(ob["scan_mask"])
+                         + len(ob["row_arr"]) * 4 + 16 * 40 + n * xb + m * xb)
+                out.append((f"{fmt}_{p}", O.OracleMatrix(ob), b, dt))
     return out
 
 
@@ -389,7 +474,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference scalar library not built (make -C oracle ref)"}))
         return
     m, n, Rst, Col, Val = workload(args.workload, args.n)
-    precs = [p if p != "mixed" else "f32" for p in args.precisions.split(",")]
+    precs = args.precisions.split(",")
     cases = cpu_cases(m, n, Rst, Col, Val, args.formats.split(","), precs)
     x = np.random.default_rng(0).uniform(-1, 1, n)
     for _ in range(max(args.warmup, 1)):
@@ -426,7 +511,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="powerlaw", choices=["powerlaw", "stencil", "laplace"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
-    ap.add_argument("--formats", default="crs,hcsr,csr5")
+    ap.add_argument("--formats", default="crs,hcsr,csr5,sell,lav,vnec,vhcc,cvr")
     ap.add_argument("--precisions", default="f64,f32,mixed")
     ap.add_argument("--cpu-iters", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -169,6 +169,237 @@ int rvvla_hcsr_spmv_f32(const rvvla_hcsr* A, float alpha, const float* x, float 
 int rvvla_hcsr_spmv_mixed(const rvvla_hcsr* A, int val_type, float alpha, const float* x,
                           float beta, float* y, void* stream);
 
+/* ------------------------------------------------------------ SELL-C-sigma
+ * spMtxSELL_C_Sigma<T> (include/SELL_C_Sigma.h:23-40): m, n, cnt_b, nz, C,
+ * Sigma, vCl/vCs/vBs/vSBs[cnt_b], vCol/vVal[len], vPerm[m]. */
+typedef struct rvvla_sell {
+  int64_t m, n, cnt_b, nz;
+  int32_t C, Sigma;
+  const int32_t* vCl;
+  const int32_t* vCs;
+  const int32_t* vBs;
+  const int32_t* vSBs;
+  const uint32_t* vCol;
+  const uint32_t* vPerm;
+  const void* vVal;
+  int64_t len;
+} rvvla_sell;
+
+typedef struct rvvla_sell_owned {
+  rvvla_sell h;
+  int32_t *vCl, *vCs, *vBs, *vSBs;
+  uint32_t *vCol, *vPerm;
+  void* vVal;
+} rvvla_sell_owned;
+
+/* Builder (the reference has none): rows sorted by length, descending and
+ * stable, inside windows of sigma rows; slices of C rows; column-major slice
+ * storage padded with value 0 / column 0.  Synchronises `stream`. */
+int rvvla_sell_build(const rvvla_crs* src, int val_bytes, int64_t C, int64_t sigma,
+                     rvvla_sell_owned* out, void* stream);
+void rvvla_sell_free(rvvla_sell_owned* h);
+/* sparse_mv<double, spMtxSELL_C_Sigma, *, stage> —
+ * src/scalar/spmv_mtx_sell_c_sigma.cpp:22-149; stage is an rvvla_stage. */
+int rvvla_sell_spmv_f64(const rvvla_sell* A, int stage, double alpha, const double* x, double beta,
+                        double* y, void* stream);
+/* sparse_mv<float, spMtxSELL_C_Sigma, *, stage> —
+ * src/scalar/spmv_mtx_sell_c_sigma.cpp:151-275 */
+int rvvla_sell_spmv_f32(const rvvla_sell* A, int stage, float alpha, const float* x, float beta,
+                        float* y, void* stream);
+/* Mixed precision, all stages (no reference counterpart). */
+int rvvla_sell_spmv_mixed(const rvvla_sell* A, int val_type, float alpha, const float* x,
+                          float beta, float* y, void* stream);
+
+/* ------------------------------------------------------------ LAV
+ * spMtxLAV<T> (include/LAV.h:11-31): SIMD_Lanes, m, n, nz, segment_count,
+ * chunk_count, T, segment_len, chunk_offsets[(chunk_count+1)*segment_count],
+ * chunk_offsets_full_mask[chunk_count*segment_count],
+ * segment_ptr[segment_count+1], out_order[segment_count*chunk_count*SIMD_Lanes],
+ * mask[n_steps], val/col_id[n_steps*SIMD_Lanes] and sparse_part (CRS). */
+typedef struct rvvla_lav {
+  int64_t SIMD_Lanes, m, n, nz, segment_count, chunk_count, segment_len, n_steps;
+  double T;
+  const int32_t* chunk_offsets;
+  const int32_t* chunk_offsets_full_mask;
+  const uint64_t* segment_ptr;
+  const uint32_t* out_order;
+  const uint16_t* mask;
+  const void* val;
+  const uint32_t* col_id;
+  rvvla_crs sparse_part;
+} rvvla_lav;
+
+typedef struct rvvla_lav_owned {
+  rvvla_lav h;
+  int32_t *chunk_offsets, *chunk_offsets_full_mask;
+  uint64_t* segment_ptr;
+  uint32_t* out_order;
+  uint16_t* mask;
+  void* val;
+  uint32_t* col_id;
+  int32_t *sp_Rst, *sp_Col;
+  void* sp_Val;
+} rvvla_lav_owned;
+
+/* Builder (the reference has none; built on the host, then uploaded): dense
+ * columns = the most populated columns holding >= (1-T) of the nonzeros,
+ * segments of segment_len of them; rows chunked by dense count, descending;
+ * inside a chunk each segment orders rows by their count in that segment.
+ * Synchronises `stream`. */
+int rvvla_lav_build(const rvvla_crs* src, int val_bytes, int64_t simd_lanes, double T,
+                    int64_t segment_len, rvvla_lav_owned* out, void* stream);
+void rvvla_lav_free(rvvla_lav_owned* h);
+/* sparse_mv<double, spMtxLAV, false> — src/scalar/spmv_mtx_lav.cpp:24-85 */
+int rvvla_lav_spmv_f64(const rvvla_lav* A, double alpha, const double* x, double beta, double* y,
+                       void* stream);
+/* sparse_mv<float, spMtxLAV, false> — src/scalar/spmv_mtx_lav.cpp:87-148 */
+int rvvla_lav_spmv_f32(const rvvla_lav* A, float alpha, const float* x, float beta, float* y,
+                       void* stream);
+
+/* ------------------------------------------------------------ VNEC
+ * spMtxVNEC<T> (include/VNEC.h:35-76): the source CRS (ptr/indices/val =
+ * M.ptr/M.indices/M.val), NUM_THREADS_VNEC, vnec_t (SpB_VNEC_type: 0 D,
+ * 1 S, 2 L), IRD_mat, thread_coord_start/_end ((x, y) pairs per thread),
+ * D arrays (ecr_indices, NEC_NUM, use_x_indices (flattened, offsets
+ * use_x_ptr), v_row_ptr, col_start, val_align) and S arrays (tasks
+ * (flattened), reorder_mat.task_start/task_end/row_begin/row_end/col/nnz,
+ * spvv_len).  nLanes = nLanes_f64 (8) or nLanes_f32 (16); max_nec = largest
+ * NEC_NUM (the shared-memory size of the compacted x). */
+typedef struct rvvla_vnec {
+  int64_t m, n, nz;
+  int32_t NUM_THREADS_VNEC, nLanes, vnec_t, max_nec;
+  float IRD_mat;
+  const int32_t* ptr;
+  const int32_t* indices;
+  const void* val;
+  const int32_t* thread_coord_start;
+  const int32_t* thread_coord_end;
+  const int32_t* ecr_indices;
+  const int32_t* NEC_NUM;
+  const int32_t* use_x_ptr;
+  const int32_t* use_x_indices;
+  const int32_t* v_row_ptr;
+  const int32_t* col_start;
+  const void* val_align;
+  int64_t ngroups;
+  const int32_t* tasks;
+  const int32_t* task_start;
+  const int32_t* task_end;
+  const int32_t* spvv_len;
+  const int32_t* row_begin;
+  const int32_t* row_end;
+  const int32_t* reorder_col;
+  const void* reorder_nnz;
+  int64_t ntasks, nreorder;
+} rvvla_vnec;
+
+typedef struct rvvla_vnec_owned {
+  rvvla_vnec h;
+  int32_t *ptr, *indices;
+  void* val;
+  int32_t *thread_coord_start, *thread_coord_end, *ecr_indices, *NEC_NUM, *use_x_ptr, *use_x_indices;
+  int32_t *v_row_ptr, *col_start;
+  void* val_align;
+  int32_t *tasks, *task_start, *task_end, *spvv_len, *row_begin, *row_end, *reorder_col;
+  void* reorder_nnz;
+} rvvla_vnec_owned;
+
+/* spMtxVNEC(const spMtxCRS&) (include/VNEC.h:200-227): partition, x
+ * compaction, IRD and variant choice, plus the S/D structures the
+ * reference's kernels read (built on the host, then uploaded).  nthreads <= 0
+ * picks one merge tile (2048 items) per thread; variant -1 applies the
+ * reference's rule, 0/1/2 force D/S/L.  val_bytes 8 or 4.  Synchronises
+ * `stream`. */
+int rvvla_vnec_build(const rvvla_crs* src, int val_bytes, int64_t nthreads, int variant,
+                     rvvla_vnec_owned* out, void* stream);
+void rvvla_vnec_free(rvvla_vnec_owned* h);
+/* sparse_mv<double, spMtxVNEC, true> — src/rvv/spmv_mtx_vnec.cpp:588-657 */
+int rvvla_vnec_spmv_f64(const rvvla_vnec* A, double alpha, const double* x, double beta,
+                        double* y, void* stream);
+/* sparse_mv<float, spMtxVNEC, true> — src/rvv/spmv_mtx_vnec.cpp:659-738 */
+int rvvla_vnec_spmv_f32(const rvvla_vnec* A, float alpha, const float* x, float beta, float* y,
+                        void* stream);
+
+/* ------------------------------------------------------------ VHCC
+ * spMtxVHCC<T> (include/VHCC.h:15-60): vhcc_params (num_threads,
+ * num_panels, tile_row, tile_col, vec_size, n_masks), _num_rows, _num_cols,
+ * _num_entries, _num_vectors, _pad_entries, _pad_rows, _thr_info
+ * (num_threads x 10 ints: vbase, rbase, sbase, last_row, overflow_row,
+ * start_vec, end_vec, panel_id, merge_start, merge_end), _veceor_ptr
+ * (n_eor entries incl. the sentinel), _scan_mask (bytes), _row_arr,
+ * _col_arr, _vals_arr (num_vectors*vec_size). */
+typedef struct rvvla_vhcc {
+  int64_t num_rows, num_cols, num_entries, num_vectors, pad_entries, pad_rows;
+  int32_t num_threads, num_panels, tile_row, tile_col, vec_size, n_masks;
+  const int32_t* thr_info;
+  const uint32_t* veceor_ptr;
+  int64_t n_eor;
+  const uint8_t* scan_mask;
+  int64_t scan_mask_bytes;
+  const uint32_t* row_arr;
+  int64_t n_rowarr;
+  const uint32_t* col_arr;
+  const void* vals_arr;
+} rvvla_vhcc;
+
+typedef struct rvvla_vhcc_owned {
+  rvvla_vhcc h;
+  int32_t* thr_info;
+  uint32_t* veceor_ptr;
+  uint8_t* scan_mask;
+  uint32_t *row_arr, *col_arr;
+  void* vals_arr;
+} rvvla_vhcc_owned;
+
+/* Builder (the reference has only setters, include/VHCC.h:80-112): one
+ * panel, vec_size 32 (one vector lane per warp lane), num_threads equal
+ * vector ranges (<= 0: 64 vectors each).  Synchronises `stream`. */
+int rvvla_vhcc_build(const rvvla_crs* src, int val_bytes, int64_t num_threads, rvvla_vhcc_owned* out,
+                     void* stream);
+void rvvla_vhcc_free(rvvla_vhcc_owned* h);
+/* sparse_mv<double, spMtxVHCC, true> — src/rvv/spmv_vhcc.cpp:320-434 */
+int rvvla_vhcc_spmv_f64(const rvvla_vhcc* A, double alpha, const double* x, double beta,
+                        double* y, void* stream);
+/* sparse_mv<float, spMtxVHCC, true> — src/rvv/spmv_vhcc.cpp:252-316 */
+int rvvla_vhcc_spmv_f32(const rvvla_vhcc* A, float alpha, const float* x, float beta, float* y,
+                        void* stream);
+
+/* ------------------------------------------------------------ CVR
+ * spMtxCVR<T> (include/CVR.h:22-37): nItems, numRows, numCols, SIMD_LEN,
+ * Nthreads, Nthreads_avail, vPack_vec_vals/cols (nItems),
+ * vPack_vec_record (n_record ints: (pos, row) pairs + one trailing pair),
+ * writeback_pos_record (n_writeback = Nthreads_avail*(SIMD_LEN+2) ints). */
+typedef struct rvvla_cvr {
+  int64_t nItems, numRows, numCols;
+  int32_t SIMD_LEN, Nthreads, Nthreads_avail, no_empty_rows;
+  const void* vPack_vec_vals;
+  const uint32_t* vPack_vec_cols;
+  const int32_t* vPack_vec_record;
+  int64_t n_record;
+  const int32_t* writeback_pos_record;
+  int64_t n_writeback;
+} rvvla_cvr;
+
+typedef struct rvvla_cvr_owned {
+  rvvla_cvr h;
+  void* vPack_vec_vals;
+  uint32_t* vPack_vec_cols;
+  int32_t *vPack_vec_record, *writeback_pos_record;
+} rvvla_cvr_owned;
+
+/* Builder (the reference has none): SIMD_LEN 32; nthreads whole-row
+ * ranges balanced by nonzeros (<= 0: 2048 nonzeros each); rows enter lanes
+ * longest first.  Synchronises `stream`. */
+int rvvla_cvr_build(const rvvla_crs* src, int val_bytes, int64_t nthreads, rvvla_cvr_owned* out,
+                    void* stream);
+void rvvla_cvr_free(rvvla_cvr_owned* h);
+/* sparse_mv<double, spMtxCVR, false> — src/scalar/spmv_mtx_cvr.cpp:21-68 */
+int rvvla_cvr_spmv_f64(const rvvla_cvr* A, double alpha, const double* x, double beta, double* y,
+                       void* stream);
+/* sparse_mv<float, spMtxCVR, false> — src/scalar/spmv_mtx_cvr.cpp:70-118 */
+int rvvla_cvr_spmv_f32(const rvvla_cvr* A, float alpha, const float* x, float beta, float* y,
+                       void* stream);
+
 /* ------------------------------------------------------------ CSR5
  * spMtxCSR5<T> (include/CSR5.h:57-88): _m, _n, _nnz, _bit_y_offset,
  * _bit_seg_offset, _tile_desc_len, _tail_tile_start, _p, _omega, _sigma,

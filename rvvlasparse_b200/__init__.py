@@ -22,7 +22,12 @@ from .formats import (  # noqa: F401
     sparse_mv_mixed,
     spMtxCRS,
     spMtxCSR5,
+    spMtxCVR,
     spMtxHCSR,
+    spMtxLAV,
+    spMtxSELL_C_Sigma,
+    spMtxVHCC,
+    spMtxVNEC,
 )
 
 __version__ = "0.1.0"

@@ -45,6 +45,72 @@ class rvvla_crs(C.Structure):
                 ("plan_tiles", i64), ("plan_kind", i32)]
 
 
+class rvvla_sell(C.Structure):
+    _fields_ = [("m", i64), ("n", i64), ("cnt_b", i64), ("nz", i64), ("C", i32), ("Sigma", i32), ("vCl", vp),
+                ("vCs", vp), ("vBs", vp), ("vSBs", vp), ("vCol", vp), ("vPerm", vp), ("vVal", vp), ("len", i64)]
+
+
+class rvvla_sell_owned(C.Structure):
+    _fields_ = [("h", rvvla_sell), ("vCl", vp), ("vCs", vp), ("vBs", vp), ("vSBs", vp), ("vCol", vp),
+                ("vPerm", vp), ("vVal", vp)]
+
+
+VNEC_ARRAYS = ("ptr", "indices", "val", "thread_coord_start", "thread_coord_end", "ecr_indices", "NEC_NUM",
+               "use_x_ptr", "use_x_indices", "v_row_ptr", "col_start", "val_align", "tasks", "task_start",
+               "task_end", "spvv_len", "row_begin", "row_end", "reorder_col", "reorder_nnz")
+
+
+class rvvla_lav(C.Structure):
+    _fields_ = [("SIMD_Lanes", i64), ("m", i64), ("n", i64), ("nz", i64), ("segment_count", i64),
+                ("chunk_count", i64), ("segment_len", i64), ("n_steps", i64), ("T", dbl), ("chunk_offsets", vp),
+                ("chunk_offsets_full_mask", vp), ("segment_ptr", vp), ("out_order", vp), ("mask", vp), ("val", vp),
+                ("col_id", vp), ("sparse_part", rvvla_crs)]
+
+
+class rvvla_lav_owned(C.Structure):
+    _fields_ = [("h", rvvla_lav), ("chunk_offsets", vp), ("chunk_offsets_full_mask", vp), ("segment_ptr", vp),
+                ("out_order", vp), ("mask", vp), ("val", vp), ("col_id", vp), ("sp_Rst", vp), ("sp_Col", vp),
+                ("sp_Val", vp)]
+
+
+class rvvla_vnec(C.Structure):
+    _fields_ = [("m", i64), ("n", i64), ("nz", i64), ("NUM_THREADS_VNEC", i32), ("nLanes", i32), ("vnec_t", i32),
+                ("max_nec", i32), ("IRD_mat", flt), ("ptr", vp), ("indices", vp), ("val", vp),
+                ("thread_coord_start", vp), ("thread_coord_end", vp), ("ecr_indices", vp), ("NEC_NUM", vp),
+                ("use_x_ptr", vp), ("use_x_indices", vp), ("v_row_ptr", vp), ("col_start", vp),
+                ("val_align", vp), ("ngroups", i64), ("tasks", vp), ("task_start", vp), ("task_end", vp),
+                ("spvv_len", vp), ("row_begin", vp), ("row_end", vp), ("reorder_col", vp), ("reorder_nnz", vp),
+                ("ntasks", i64), ("nreorder", i64)]
+
+
+class rvvla_vnec_owned(C.Structure):
+    _fields_ = [("h", rvvla_vnec)] + [(k, vp) for k in VNEC_ARRAYS]
+
+
+class rvvla_vhcc(C.Structure):
+    _fields_ = [("num_rows", i64), ("num_cols", i64), ("num_entries", i64), ("num_vectors", i64),
+                ("pad_entries", i64), ("pad_rows", i64), ("num_threads", i32), ("num_panels", i32),
+                ("tile_row", i32), ("tile_col", i32), ("vec_size", i32), ("n_masks", i32), ("thr_info", vp),
+                ("veceor_ptr", vp), ("n_eor", i64), ("scan_mask", vp), ("scan_mask_bytes", i64), ("row_arr", vp),
+                ("n_rowarr", i64), ("col_arr", vp), ("vals_arr", vp)]
+
+
+class rvvla_vhcc_owned(C.Structure):
+    _fields_ = [("h", rvvla_vhcc), ("thr_info", vp), ("veceor_ptr", vp), ("scan_mask", vp), ("row_arr", vp),
+                ("col_arr", vp), ("vals_arr", vp)]
+
+
+class rvvla_cvr(C.Structure):
+    _fields_ = [("nItems", i64), ("numRows", i64), ("numCols", i64), ("SIMD_LEN", i32), ("Nthreads", i32),
+                ("Nthreads_avail", i32), ("no_empty_rows", i32), ("vPack_vec_vals", vp), ("vPack_vec_cols", vp),
+                ("vPack_vec_record", vp), ("n_record", i64), ("writeback_pos_record", vp), ("n_writeback", i64)]
+
+
+class rvvla_cvr_owned(C.Structure):
+    _fields_ = [("h", rvvla_cvr), ("vPack_vec_vals", vp), ("vPack_vec_cols", vp), ("vPack_vec_record", vp),
+                ("writeback_pos_record", vp)]
+
+
 class rvvla_csr5(C.Structure):
     _fields_ = [("m", i64), ("n", i64), ("nnz", i64), ("bit_y_offset", i32), ("bit_seg_offset", i32),
                 ("tile_desc_len", i32), ("tail_tile_start", i32), ("p", i32), ("omega", i32), ("sigma", i32),
@@ -109,6 +175,32 @@ def load():
     _proto(lib, "rvvla_hcsr_spmv_f64", cint, P(rvvla_hcsr), dbl, vp, dbl, vp, vp)
     _proto(lib, "rvvla_hcsr_spmv_f32", cint, P(rvvla_hcsr), flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_hcsr_spmv_mixed", cint, P(rvvla_hcsr), cint, flt, vp, flt, vp, vp)
+    # SELL-C-sigma
+    _proto(lib, "rvvla_sell_build", cint, P(rvvla_crs), cint, i64, i64, P(rvvla_sell_owned), vp)
+    _proto(lib, "rvvla_sell_free", None, P(rvvla_sell_owned))
+    _proto(lib, "rvvla_sell_spmv_f64", cint, P(rvvla_sell), cint, dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_sell_spmv_f32", cint, P(rvvla_sell), cint, flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_sell_spmv_mixed", cint, P(rvvla_sell), cint, flt, vp, flt, vp, vp)
+    # LAV
+    _proto(lib, "rvvla_lav_build", cint, P(rvvla_crs), cint, i64, dbl, i64, P(rvvla_lav_owned), vp)
+    _proto(lib, "rvvla_lav_free", None, P(rvvla_lav_owned))
+    _proto(lib, "rvvla_lav_spmv_f64", cint, P(rvvla_lav), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_lav_spmv_f32", cint, P(rvvla_lav), flt, vp, flt, vp, vp)
+    # VNEC
+    _proto(lib, "rvvla_vnec_build", cint, P(rvvla_crs), cint, i64, cint, P(rvvla_vnec_owned), vp)
+    _proto(lib, "rvvla_vnec_free", None, P(rvvla_vnec_owned))
+    _proto(lib, "rvvla_vnec_spmv_f64", cint, P(rvvla_vnec), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_vnec_spmv_f32", cint, P(rvvla_vnec), flt, vp, flt, vp, vp)
+    # VHCC
+    _proto(lib, "rvvla_vhcc_build", cint, P(rvvla_crs), cint, i64, P(rvvla_vhcc_owned), vp)
+    _proto(lib, "rvvla_vhcc_free", None, P(rvvla_vhcc_owned))
+    _proto(lib, "rvvla_vhcc_spmv_f64", cint, P(rvvla_vhcc), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_vhcc_spmv_f32", cint, P(rvvla_vhcc), flt, vp, flt, vp, vp)
+    # CVR
+    _proto(lib, "rvvla_cvr_build", cint, P(rvvla_crs), cint, i64, P(rvvla_cvr_owned), vp)
+    _proto(lib, "rvvla_cvr_free", None, P(rvvla_cvr_owned))
+    _proto(lib, "rvvla_cvr_spmv_f64", cint, P(rvvla_cvr), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_cvr_spmv_f32", cint, P(rvvla_cvr), flt, vp, flt, vp, vp)
     # CSR5
     _proto(lib, "rvvla_csr5_build", cint, P(rvvla_crs), cint, cint, cint, P(rvvla_csr5_owned), vp)
     _proto(lib, "rvvla_csr5_free", None, P(rvvla_csr5_owned))

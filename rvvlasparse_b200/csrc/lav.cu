@@ -1,0 +1,169 @@
+// lav.cu — spMtxLAV on sm_100a: builder (host, then uploaded) and SpMV.
+//
+// Layout (include/LAV.h:10-31 of the reference) as read by
+// src/scalar/spmv_mtx_lav.cpp:36-79: dense columns cut into segments; per
+// segment, chunks of SIMD_Lanes rows (out_order), each chunk a run of steps
+// (chunk_offsets, relative to segment_ptr[s]); steps before
+// chunk_offsets_full_mask use every lane, later ones mask[step] lanes (a
+// prefix); val/col_id lane-major per step; the remaining entries in
+// sparse_part (CRS, which applies beta to every row).  The reference ships no
+// builder; this one reproduces the oracle's: dense columns = the densest
+// columns holding >= (1-T) of the nonzeros, segments of segment_len columns
+// in density order, one global row chunking (rows by dense count,
+// descending) with each segment ordering a chunk's rows by their count in
+// that segment.
+//
+// SpMV: sparse part through the CRS kernels (with its analysis plan), then
+// one launch per segment (the reference's segment loop, :147-174): a thread
+// per (chunk, lane) sums its steps and adds alpha*sum to y[out_order]; a row
+// appears once per segment, so the launches need no atomics.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "crs_merge.cuh"
+#include "lav_build.h"
+#include "rvvla_internal.cuh"
+
+extern "C" int rvvla_crs_spmv_f64(const rvvla_crs*, double, const double*, double, double*, void*);
+extern "C" int rvvla_crs_spmv_f32(const rvvla_crs*, float, const float*, float, float*, void*);
+
+namespace rvvla {
+namespace {
+
+template <class V, class X, class CT>
+__global__ void __launch_bounds__(256)
+lav_segment_kernel(int64_t s, int64_t L, int64_t cc, const int* __restrict__ co, const int* __restrict__ cf,
+                   const uint64_t* __restrict__ sp, const uint32_t* __restrict__ oo, const uint16_t* __restrict__ mk,
+                   const V* __restrict__ val, const uint32_t* __restrict__ col, const X* __restrict__ x,
+                   X* __restrict__ y, X alpha) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= cc * L) return;
+  const int64_t c = gid / L, i = gid - c * L;
+  const int64_t sh = (cc + 1) * s;
+  const int st = co[sh + c], en = co[sh + c + 1], fe = cf[s * cc + c];
+  if (st >= en) return;
+  const int64_t base = (int64_t)sp[s];
+  const bool active = (fe > st) || (i < (int64_t)mk[base + st]);
+  if (!active) return;
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+  CT acc = 0;
+  for (int q = st; q < fe; ++q) {
+    const int64_t e = (base + q) * L + i;
+    acc += (CT)vmul(ld_stream(val + e, pf), ld_keep(x + ld_stream(col + e, pf), pl));
+  }
+  for (int q = fe; q < en; ++q) {
+    if (i >= (int64_t)mk[base + q]) break;  // masks are non-increasing
+    const int64_t e = (base + q) * L + i;
+    acc += (CT)vmul(ld_stream(val + e, pf), ld_keep(x + ld_stream(col + e, pf), pl));
+  }
+  const uint32_t r = oo[(c + cc * s) * L + i];
+  y[r] += alpha * (X)acc;
+}
+
+template <class T>
+int upload(const std::vector<T>& v, T** dst, cudaStream_t st) {
+  RVVLA_CUDA(cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)));
+  if (!v.empty()) RVVLA_CUDA(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return RVVLA_OK;
+}
+
+template <class T>
+int lav_build_typed(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen, rvvla_lav_owned* out, cudaStream_t st) {
+  const int64_t m = src->m, nz = src->nz;
+  std::vector<int> Rst((size_t)m + 1), Col((size_t)nz);
+  std::vector<T> Val((size_t)nz);
+  RVVLA_CUDA(cudaMemcpyAsync(Rst.data(), src->Rst, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (nz) {
+    RVVLA_CUDA(cudaMemcpyAsync(Col.data(), src->Col, nz * sizeof(int), cudaMemcpyDeviceToHost, st));
+    RVVLA_CUDA(cudaMemcpyAsync(Val.data(), src->Val, nz * sizeof(T), cudaMemcpyDeviceToHost, st));
+  }
+  RVVLA_CUDA(cudaStreamSynchronize(st));
+  LavHost<T> H;
+  lav_build_host<T>(Rst.data(), Col.data(), Val.data(), m, src->n, nz, L, Tthr, seglen, H);
+  rvvla_lav& h = out->h;
+  h.SIMD_Lanes = L; h.m = m; h.n = src->n; h.nz = nz; h.segment_count = H.nseg; h.chunk_count = H.cc;
+  h.segment_len = seglen; h.T = Tthr; h.n_steps = (int64_t)H.mk.size();
+  int rc = 0;
+  if ((rc = upload(H.co, &out->chunk_offsets, st)) || (rc = upload(H.cf, &out->chunk_offsets_full_mask, st)) ||
+      (rc = upload(H.sp, &out->segment_ptr, st)) || (rc = upload(H.oo, &out->out_order, st)) ||
+      (rc = upload(H.mk, &out->mask, st)) || (rc = upload(H.val, reinterpret_cast<T**>(&out->val), st)) ||
+      (rc = upload(H.col, &out->col_id, st)) || (rc = upload(H.sRst, &out->sp_Rst, st)) ||
+      (rc = upload(H.sCol, &out->sp_Col, st)) || (rc = upload(H.sVal, reinterpret_cast<T**>(&out->sp_Val), st)))
+    return rc;
+  h.chunk_offsets = out->chunk_offsets; h.chunk_offsets_full_mask = out->chunk_offsets_full_mask;
+  h.segment_ptr = out->segment_ptr; h.out_order = out->out_order; h.mask = out->mask; h.val = out->val;
+  h.col_id = out->col_id;
+  h.sparse_part.m = m; h.sparse_part.n = src->n; h.sparse_part.nz = (int64_t)H.sCol.size();
+  h.sparse_part.Rst = out->sp_Rst; h.sparse_part.Col = out->sp_Col; h.sparse_part.Val = out->sp_Val;
+  h.sparse_part.plan = nullptr; h.sparse_part.plan_tiles = 0; h.sparse_part.plan_kind = 0;
+  RVVLA_CUDA(cudaStreamSynchronize(st));
+  return RVVLA_OK;
+}
+
+template <class V, class X, class CT>
+int lav_spmv_impl(const rvvla_lav* A, X alpha, const X* x, X beta, X* y, cudaStream_t st,
+                  int (*crs_fn)(const rvvla_crs*, X, const X*, X, X*, void*)) {
+  if (!A) return fail(RVVLA_ERR_INVALID_ARG, "lav: null descriptor");
+  if (A->m < 0 || A->SIMD_Lanes <= 0 || A->segment_count < 0 || A->chunk_count != (A->m + A->SIMD_Lanes - 1) / A->SIMD_Lanes)
+    return fail(RVVLA_ERR_INVALID_ARG, "lav: bad sizes");
+  if (A->m == 0) return RVVLA_OK;
+  // sparse part: y = alpha*S*x + beta*y over every row (spmv_mtx_lav.cpp:31)
+  int rc = crs_fn(&A->sparse_part, alpha, x, beta, y, (void*)st);
+  if (rc) return rc;
+  const int64_t threads = A->chunk_count * A->SIMD_Lanes;
+  for (int64_t s = 0; s < A->segment_count; ++s) {
+    lav_segment_kernel<V, X, CT><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+        s, A->SIMD_Lanes, A->chunk_count, A->chunk_offsets, A->chunk_offsets_full_mask, A->segment_ptr, A->out_order,
+        A->mask, (const V*)A->val, A->col_id, x, y, alpha);
+    RVVLA_LAUNCHED("lav_segment_kernel");
+  }
+  return RVVLA_OK;
+}
+
+}  // namespace
+}  // namespace rvvla
+
+using namespace rvvla;
+
+extern "C" {
+
+int rvvla_lav_build(const rvvla_crs* src, int val_bytes, int64_t simd_lanes, double T, int64_t segment_len,
+                    rvvla_lav_owned* out, void* stream) {
+  if (!src || !out) return fail(RVVLA_ERR_INVALID_ARG, "lav_build: null argument");
+  std::memset(out, 0, sizeof(*out));
+  if (simd_lanes <= 0 || segment_len <= 0 || simd_lanes > 65535)
+    return fail(RVVLA_ERR_INVALID_ARG, "LAV: SIMD_Lanes and segment_len must be positive");
+  if (src->m < 0 || src->n < 0 || src->nz < 0) return fail(RVVLA_ERR_INVALID_ARG, "lav_build: bad sizes");
+  int rc;
+  if (val_bytes == 8) rc = lav_build_typed<double>(src, simd_lanes, T, segment_len, out, as_stream(stream));
+  else if (val_bytes == 4) rc = lav_build_typed<float>(src, simd_lanes, T, segment_len, out, as_stream(stream));
+  else rc = fail(RVVLA_ERR_INVALID_ARG, "lav_build: val_bytes must be 8 or 4");
+  if (rc) {
+    std::string keep = rvvla_last_error();
+    rvvla_lav_free(out);
+    set_error(keep);
+  }
+  return rc;
+}
+
+void rvvla_lav_free(rvvla_lav_owned* h) {
+  if (!h) return;
+  void* ptrs[] = {h->chunk_offsets, h->chunk_offsets_full_mask, h->segment_ptr, h->out_order, h->mask, h->val,
+                  h->col_id, h->sp_Rst, h->sp_Col, h->sp_Val};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  std::memset(h, 0, sizeof(*h));
+}
+
+int rvvla_lav_spmv_f64(const rvvla_lav* A, double alpha, const double* x, double beta, double* y, void* stream) {
+  return lav_spmv_impl<double, double, double>(A, alpha, x, beta, y, as_stream(stream), rvvla_crs_spmv_f64);
+}
+
+int rvvla_lav_spmv_f32(const rvvla_lav* A, float alpha, const float* x, float beta, float* y, void* stream) {
+  return lav_spmv_impl<float, float, float>(A, alpha, x, beta, y, as_stream(stream), rvvla_crs_spmv_f32);
+}
+
+}  // extern "C"

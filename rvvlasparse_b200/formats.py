@@ -217,6 +217,253 @@ def _hcsr_convert(dist: spMtxHCSR, src: spMtxCRS, params: convertParams) -> None
         lib.rvvla_hcsr_free(C.byref(owned))
 
 
+# ------------------------------------------------------------------ generic
+
+
+class _GpuFormat:
+    """Mirror of a reference format class: scalar fields + CUDA arrays.
+    Subclasses list SCALARS, ARRAYS (name -> torch dtype, None = value type),
+    the ctypes descriptor type and the value array's name."""
+
+    SCALARS: tuple = ()
+    ARRAYS: dict = {}
+    CDESC = None
+    VALUE = ""
+
+    def __init__(self):
+        for k in self.SCALARS:
+            setattr(self, k, 0)
+        for k in self.ARRAYS:
+            setattr(self, k, None)
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return getattr(self, self.VALUE).dtype
+
+    def astype(self, dtype: torch.dtype):
+        c = type(self)()
+        c.__dict__.update(self.__dict__)
+        setattr(c, self.VALUE, getattr(self, self.VALUE).to(dtype))
+        return c
+
+    def desc(self):
+        d = self.CDESC()
+        for k in self.SCALARS:
+            if hasattr(d, k):
+                setattr(d, k, int(getattr(self, k)))
+        for k in self.ARRAYS:
+            if hasattr(d, k):
+                setattr(d, k, _ptr(getattr(self, k)))
+        return d
+
+    def to_host(self) -> dict:
+        out = {k: int(getattr(self, k)) for k in self.SCALARS}
+        for k in self.ARRAYS:
+            a = getattr(self, k)
+            if a is not None:
+                out[k] = a.cpu().numpy()
+        return out
+
+    def _adopt(self, owned, sizes: dict, value_dtype, device) -> None:
+        h = owned.h
+        for k in self.SCALARS:
+            if hasattr(h, k):
+                setattr(self, k, int(getattr(h, k)))
+        for k, n in sizes.items():
+            dt = self.ARRAYS[k] or value_dtype
+            setattr(self, k, _owned_to_tensor(getattr(owned, k), int(n), dt, device))
+
+
+def _build(lib_fn, free_fn, owned, *args):
+    st = lib_fn(*args, C.byref(owned), _stream())
+    if st != 0:
+        msg = load().rvvla_last_error().decode()
+        raise (ValueError if st == _capi.RVVLA_ERR_INVALID_ARG else RuntimeError)(msg)
+
+
+class spMtxSELL_C_Sigma(_GpuFormat):
+    """``spMtxSELL_C_Sigma<ValT>`` (include/SELL_C_Sigma.h:23-40)."""
+
+    SCALARS = ("m", "n", "cnt_b", "nz", "C", "Sigma", "len")
+    ARRAYS = {"vCl": torch.int32, "vCs": torch.int32, "vBs": torch.int32, "vSBs": torch.int32,
+              "vCol": torch.int32, "vPerm": torch.int32, "vVal": None}
+    CDESC = _capi.rvvla_sell
+    VALUE = "vVal"
+
+
+def _sell_convert(dist, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    owned = _capi.rvvla_sell_owned()
+    Cc = int(params.param.get("C", 32))
+    sigma = int(params.param.get("sigma", params.param.get("Sigma", 256)))
+    _build(lib.rvvla_sell_build, lib.rvvla_sell_free, owned, C.byref(src.desc()), src.Val.element_size(), Cc, sigma)
+    try:
+        h = owned.h
+        sizes = {"vCl": h.cnt_b, "vCs": h.cnt_b, "vBs": h.cnt_b, "vSBs": h.cnt_b, "vCol": h.len, "vPerm": h.m,
+                 "vVal": h.len}
+        dist._adopt(owned, sizes, src.Val.dtype, src.Val.device)
+    finally:
+        lib.rvvla_sell_free(C.byref(owned))
+
+
+class spMtxVNEC(_GpuFormat):
+    """``spMtxVNEC<ValT>`` (include/VNEC.h:35-76).  Unlike the reference (which
+    keeps a pointer to the source CRS), the source arrays are copied in."""
+
+    SCALARS = ("m", "n", "nz", "NUM_THREADS_VNEC", "nLanes", "vnec_t", "max_nec", "ngroups", "ntasks", "nreorder")
+    ARRAYS = {k: (None if k in ("val", "val_align", "reorder_nnz") else torch.int32) for k in _capi.VNEC_ARRAYS}
+    CDESC = _capi.rvvla_vnec
+    VALUE = "val"
+
+    def astype(self, dtype):
+        c = super().astype(dtype)
+        for k in ("val_align", "reorder_nnz"):
+            if getattr(self, k) is not None:
+                setattr(c, k, getattr(self, k).to(dtype))
+        return c
+
+
+def _vnec_convert(dist, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    owned = _capi.rvvla_vnec_owned()
+    nt = int(params.param.get("NUM_THREADS_VNEC", params.param.get("threads", 0)))
+    variant = int(params.param.get("variant", -1))
+    _build(lib.rvvla_vnec_build, lib.rvvla_vnec_free, owned, C.byref(src.desc()), src.Val.element_size(), nt, variant)
+    try:
+        h = owned.h
+        NT = h.NUM_THREADS_VNEC
+        sizes = {"ptr": h.m + 1, "indices": h.nz, "val": h.nz, "thread_coord_start": 2 * NT,
+                 "thread_coord_end": 2 * NT}
+        if h.vnec_t == 0:
+            sizes.update({"ecr_indices": h.nz, "NEC_NUM": NT, "use_x_ptr": NT + 1, "v_row_ptr": h.m + 1,
+                          "col_start": h.ngroups, "val_align": h.ngroups * h.nLanes})
+        elif h.vnec_t == 1:
+            sizes.update({"NEC_NUM": NT, "use_x_ptr": NT + 1, "tasks": h.ntasks, "task_start": NT, "task_end": NT,
+                          "spvv_len": NT, "row_begin": h.ntasks, "row_end": h.ntasks, "reorder_col": h.nreorder,
+                          "reorder_nnz": h.nreorder})
+        if h.vnec_t in (0, 1):
+            # use_x_indices length = use_x_ptr[NT]: read it back
+            tmp = _owned_to_tensor(owned.use_x_ptr, NT + 1, torch.int32, src.Val.device)
+            sizes["use_x_indices"] = int(tmp[-1].item())
+        dist._adopt(owned, sizes, src.Val.dtype, src.Val.device)
+        dist.IRD_mat = float(h.IRD_mat)
+    finally:
+        lib.rvvla_vnec_free(C.byref(owned))
+
+
+class spMtxLAV(_GpuFormat):
+    """``spMtxLAV<ValT>`` (include/LAV.h:11-31); ``sparse_part`` is an
+    :class:`spMtxCRS` on the same device."""
+
+    SCALARS = ("SIMD_Lanes", "m", "n", "nz", "segment_count", "chunk_count", "segment_len", "n_steps")
+    ARRAYS = {"chunk_offsets": torch.int32, "chunk_offsets_full_mask": torch.int32, "segment_ptr": torch.int64,
+              "out_order": torch.int32, "mask": torch.int16, "val": None, "col_id": torch.int32}
+    CDESC = _capi.rvvla_lav
+    VALUE = "val"
+
+    def __init__(self):
+        super().__init__()
+        self.T = 0.2
+        self.sparse_part = None
+
+    def astype(self, dtype: torch.dtype):
+        c = super().astype(dtype)
+        c.sparse_part = self.sparse_part.astype(dtype)
+        return c
+
+    def desc(self):
+        d = super().desc()
+        d.T = float(self.T)
+        d.sparse_part = self.sparse_part.desc(
+            _capi.RVVLA_F64 if self.sparse_part.dtype == torch.float64 else _capi.RVVLA_F32)
+        return d
+
+    def to_host(self) -> dict:
+        out = super().to_host()
+        out["T"] = float(self.T)
+        out["mask"] = out["mask"].view(np.uint16)
+        out["segment_ptr"] = out["segment_ptr"].view(np.uint64)
+        sp = self.sparse_part
+        out.update(sparse_nz=sp.nz, sp_Rst=sp.Rst.cpu().numpy(), sp_Col=sp.Col.cpu().numpy(),
+                   sp_Val=sp.Val.cpu().numpy())
+        return out
+
+
+def _lav_convert(dist, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    owned = _capi.rvvla_lav_owned()
+    lanes = int(params.param.get("SIMD_Lanes", 8))
+    T = float(params.param.get("T", 0.2))
+    seglen = int(params.param.get("segment_len", 40000))
+    _build(lib.rvvla_lav_build, lib.rvvla_lav_free, owned, C.byref(src.desc()), src.Val.element_size(), lanes, T,
+           seglen)
+    try:
+        h = owned.h
+        L, cc, ns = h.SIMD_Lanes, h.chunk_count, h.segment_count
+        sizes = {"chunk_offsets": (cc + 1) * ns, "chunk_offsets_full_mask": cc * ns, "segment_ptr": ns + 1,
+                 "out_order": ns * cc * L, "mask": h.n_steps, "val": h.n_steps * L, "col_id": h.n_steps * L}
+        dist._adopt(owned, sizes, src.Val.dtype, src.Val.device)
+        dist.T = float(h.T)
+        dev = src.Val.device
+        snz = int(h.sparse_part.nz)
+        dist.sparse_part = spMtxCRS(h.m, h.n, snz, _owned_to_tensor(owned.sp_Rst, h.m + 1, torch.int32, dev),
+                                    _owned_to_tensor(owned.sp_Col, snz, torch.int32, dev),
+                                    _owned_to_tensor(owned.sp_Val, snz, src.Val.dtype, dev))
+    finally:
+        lib.rvvla_lav_free(C.byref(owned))
+
+
+class spMtxVHCC(_GpuFormat):
+    """``spMtxVHCC<ValT>`` (include/VHCC.h:43-62): the underscore fields of
+    the reference without the underscore, vhcc_params flattened."""
+
+    SCALARS = ("num_rows", "num_cols", "num_entries", "num_vectors", "pad_entries", "pad_rows", "num_threads",
+               "num_panels", "tile_row", "tile_col", "vec_size", "n_masks", "n_eor", "scan_mask_bytes", "n_rowarr")
+    ARRAYS = {"thr_info": torch.int32, "veceor_ptr": torch.int32, "scan_mask": torch.uint8, "row_arr": torch.int32,
+              "col_arr": torch.int32, "vals_arr": None}
+    CDESC = _capi.rvvla_vhcc
+    VALUE = "vals_arr"
+
+
+def _vhcc_convert(dist, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    owned = _capi.rvvla_vhcc_owned()
+    nt = int(params.param.get("num_threads", 0))
+    _build(lib.rvvla_vhcc_build, lib.rvvla_vhcc_free, owned, C.byref(src.desc()), src.Val.element_size(), nt)
+    try:
+        h = owned.h
+        sizes = {"thr_info": h.num_threads * 10, "veceor_ptr": h.n_eor, "scan_mask": h.scan_mask_bytes,
+                 "row_arr": h.n_rowarr, "col_arr": h.num_vectors * h.vec_size, "vals_arr": h.num_vectors * h.vec_size}
+        dist._adopt(owned, sizes, src.Val.dtype, src.Val.device)
+    finally:
+        lib.rvvla_vhcc_free(C.byref(owned))
+
+
+class spMtxCVR(_GpuFormat):
+    """``spMtxCVR<ValT>`` (include/CVR.h:22-37)."""
+
+    SCALARS = ("nItems", "numRows", "numCols", "SIMD_LEN", "Nthreads", "Nthreads_avail", "no_empty_rows",
+               "n_record", "n_writeback")
+    ARRAYS = {"vPack_vec_vals": None, "vPack_vec_cols": torch.int32, "vPack_vec_record": torch.int32,
+              "writeback_pos_record": torch.int32}
+    CDESC = _capi.rvvla_cvr
+    VALUE = "vPack_vec_vals"
+
+
+def _cvr_convert(dist, src: spMtxCRS, params: convertParams) -> None:
+    lib = load()
+    owned = _capi.rvvla_cvr_owned()
+    nt = int(params.param.get("Nthreads", 0))
+    _build(lib.rvvla_cvr_build, lib.rvvla_cvr_free, owned, C.byref(src.desc()), src.Val.element_size(), nt)
+    try:
+        h = owned.h
+        sizes = {"vPack_vec_vals": h.nItems, "vPack_vec_cols": h.nItems, "vPack_vec_record": h.n_record,
+                 "writeback_pos_record": h.n_writeback}
+        dist._adopt(owned, sizes, src.Val.dtype, src.Val.device)
+    finally:
+        lib.rvvla_cvr_free(C.byref(owned))
+
+
 # ------------------------------------------------------------------ CSR5
 
 
@@ -302,13 +549,43 @@ def convert(dist, src: spMtxCRS, params: convertParams | None = None):
 
 
 def _builders():
-    return {spMtxHCSR: _hcsr_convert, spMtxCSR5: _csr5_convert}
+    return {spMtxHCSR: _hcsr_convert, spMtxCSR5: _csr5_convert, spMtxSELL_C_Sigma: _sell_convert,
+            spMtxVNEC: _vnec_convert, spMtxVHCC: _vhcc_convert, spMtxCVR: _cvr_convert, spMtxLAV: _lav_convert}
 
 
-def _call_spmv(mat, alpha, b: torch.Tensor, beta, y: torch.Tensor, mixed: bool) -> int:
+def _call_spmv(mat, alpha, b: torch.Tensor, beta, y: torch.Tensor, mixed: bool,
+               stage=SPARSE_MATRIX_MV_ALL_STAGES) -> int:
     lib = load()
     st = _stream()
     vt = mat.dtype
+    if isinstance(mat, spMtxCVR):
+        if mixed:
+            return _capi.RVVLA_ERR_UNSUPPORTED
+        fn = lib.rvvla_cvr_spmv_f64 if vt == torch.float64 else lib.rvvla_cvr_spmv_f32
+        return fn(C.byref(mat.desc()), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    if isinstance(mat, spMtxLAV):
+        if mixed:
+            return _capi.RVVLA_ERR_UNSUPPORTED
+        fn = lib.rvvla_lav_spmv_f64 if vt == torch.float64 else lib.rvvla_lav_spmv_f32
+        return fn(C.byref(mat.desc()), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    if isinstance(mat, spMtxVHCC):
+        if mixed:
+            return _capi.RVVLA_ERR_UNSUPPORTED
+        fn = lib.rvvla_vhcc_spmv_f64 if vt == torch.float64 else lib.rvvla_vhcc_spmv_f32
+        return fn(C.byref(mat.desc()), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    if isinstance(mat, spMtxVNEC):
+        if mixed:
+            return _capi.RVVLA_ERR_UNSUPPORTED
+        d = mat.desc()
+        d.IRD_mat = float(getattr(mat, "IRD_mat", 0.0))
+        fn = lib.rvvla_vnec_spmv_f64 if vt == torch.float64 else lib.rvvla_vnec_spmv_f32
+        return fn(C.byref(d), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+    if isinstance(mat, spMtxSELL_C_Sigma):
+        d = mat.desc()
+        if mixed:
+            return lib.rvvla_sell_spmv_mixed(C.byref(d), _dtype_code(vt), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        fn = lib.rvvla_sell_spmv_f64 if vt == torch.float64 else lib.rvvla_sell_spmv_f32
+        return fn(C.byref(d), int(stage), float(alpha), _ptr(b), float(beta), _ptr(y), st)
     if isinstance(mat, spMtxCRS):
         if mixed:
             d = mat.desc(_capi.RVVLA_F32)
@@ -364,6 +641,8 @@ def _spmv(op, alpha, mat, descr, b, beta, y, mixed: bool, stage=SPARSE_MATRIX_MV
 def _call_stage(mat, alpha, b, beta, y, stage):
     # Formats other than SELL-C-sigma have no staged form: PREPARATION and
     # GET_RESULTS are no-ops and MULT is the whole product.
+    if isinstance(mat, spMtxSELL_C_Sigma):
+        return _call_spmv(mat, alpha, b, beta, y, False, stage)
     if stage == SPARSE_MATRIX_MV_MULT:
         return _call_spmv(mat, alpha, b, beta, y, False)
     return 0
