@@ -389,6 +389,14 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
 
     out = []
     crs = {}
+    lay = {}
+
+    def layout(fmt, dt, make):
+        # one oracle build per format (f64); the f32 layout casts its values
+        if fmt not in lay:
+            lay[fmt] = make(crs[np.float64] if np.float64 in crs else O.crs(m, n, Rst, Col, Val.astype(np.float64)))
+        return lay[fmt] if dt == np.float64 else lay[fmt].astype(dt)
+
     for fmt in formats:
         for p in precs:
             if p == "mixed" and fmt not in MIXED:
@@ -410,33 +418,33 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
             elif fmt == "csr5":
                 # the reference has CSR5 only as RVV intrinsics: time the
                 # oracle's single-threaded restatement of that kernel
-                c5 = O.build_csr5(A, 32, 16)
+                c5 = layout("csr5", dt, lambda a: O.build_csr5(a, 32, 16))
                 b = csr5_bytes(m, n, len(Col), int(c5["p"]), 32, int(c5["tile_desc_len"]), int(c5["num_offsets"]),
                                vb, xb)
                 out.append((f"csr5_{p}", O.OracleMatrix(c5), b, dt))
             elif fmt == "sell":
-                sb = O.build_sell(A, 32, 256)
-                b = int(sb["len"]) * (vb + 4) + int(sb["cnt_b"]) * 16 + m * 4 + n * xb + m * xb
+                sb = layout("sell", dt, lambda a: O.build_sell(a, 32, 256))
+                b = len(sb["vVal"]) * (vb + 4) + int(sb["cnt_b"]) * 16 + m * 4 + n * xb + m * xb
                 out.append((f"sell_{p}", O.ref_sell(sb), b, dt))
             elif fmt == "lav":
-                lb = O.build_lav(A, 8, 0.2, 40000)
+                lb = layout("lav", dt, lambda a: O.build_lav(a, 8, 0.2, 40000))
                 L, cc, ns, st = 8, int(lb["chunk_count"]), int(lb["segment_count"]), len(lb["mask"])
                 b = (st * L * (vb + 4) + st * 2 + ns * cc * L * 4 + (2 * cc + 1) * ns * 4 + (ns + 1) * 8
                      + crs_bytes(m, n, int(lb["sparse_nz"]), vb, xb))
                 out.append((f"lav_{p}", O.ref_lav(lb), b, dt))
             elif fmt == "cvr":
                 # the reference kernel runs one OpenMP thread per CVR thread block
-                cb = O.build_cvr(A, 8, O.ref_num_threads())
+                cb = layout("cvr", dt, lambda a: O.build_cvr(a, 8, O.ref_num_threads()))
                 b = len(cb["vPack_vec_vals"]) * (vb + 4) + len(cb["vPack_vec_record"]) * 4 \
                     + len(cb["writeback_pos_record"]) * 4 + n * xb + m * xb
                 out.append((f"cvr_{p}", O.ref_cvr(cb), b, dt))
             elif fmt in ("vnec", "vhcc"):
                 # RVV-only in the reference: the oracle's single-threaded port
                 if fmt == "vnec":
-                    ob = O.build_vnec(A, 16, -1)
+                    ob = layout("vnec", dt, lambda a: O.build_vnec(a, 16, -1))
                     b = crs_bytes(m, n, len(Col), vb, xb) + 16 * 16
                 else:
-                    ob = O.build_vhcc(A, 16, 8)
+                    ob = layout("vhcc", dt, lambda a: O.build_vhcc(a, 16, 8))
                     b = (len(ob["vals_arr"]) * (vb + 4) + len(ob["veceor_ptr"]) * 4 + len(ob["scan_mask"])
                          + len(ob["row_arr"]) * 4 + 16 * 40 + n * xb + m * xb)
                 out.append((f"{fmt}_{p}", O.OracleMatrix(ob), b, dt))

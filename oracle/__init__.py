@@ -89,6 +89,15 @@ class Bundle:
     def dtype(self):
         return np.float32 if int(self.scalars.get("dtype", F64)) == F32 else np.float64
 
+    def astype(self, dt) -> "Bundle":
+        """The same layout with its value arrays cast to ``dt`` (layouts
+        depend on the sparsity structure only)."""
+        src = np.dtype(self.dtype)
+        arrays = {k: (a.astype(dt) if a.dtype == src else a) for k, a in self.arrays.items()}
+        b = Bundle(self.fmt, arrays, dict(self.scalars))
+        b.scalars["dtype"] = F32 if np.dtype(dt) == np.float32 else F64
+        return b
+
     def _handle(self):
         L = _lib()
         h = L.orc_bundle_new(self.fmt.encode())

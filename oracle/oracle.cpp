@@ -652,12 +652,24 @@ Bundle* build_lav(const Crs<T>& A, int64_t L, double Tthr, int64_t seglen) {
   std::vector<uint16_t> mask;
   std::vector<T> val;
   std::vector<uint32_t> col_id;
-  // entries of each row per segment, in column order
+  // each row's dense entries ordered by segment (stable: column order inside
+  // a segment); cur[r] = the row's first entry of the current segment
+  std::vector<int64_t> dptr((size_t)m + 1, 0), cur((size_t)m);
+  std::vector<int> dk;
+  for (int64_t r = 0; r < m; ++r) {
+    const size_t b = dk.size();
+    for (int64_t k = A.Rst[r]; k < A.Rst[r + 1]; ++k)
+      if (seg_of[(size_t)A.Col[k]] >= 0) dk.push_back((int)k);
+    std::stable_sort(dk.begin() + (std::ptrdiff_t)b, dk.end(),
+                     [&](int a, int c) { return seg_of[(size_t)A.Col[a]] < seg_of[(size_t)A.Col[c]]; });
+    dptr[(size_t)r + 1] = (int64_t)dk.size();
+    cur[(size_t)r] = dptr[(size_t)r];
+  }
   std::vector<int64_t> scount((size_t)m);
   for (int64_t s = 0; s < nseg; ++s) {
     for (int64_t r = 0; r < m; ++r) {
       int64_t c = 0;
-      for (int64_t k = A.Rst[r]; k < A.Rst[r + 1]; ++k) c += (seg_of[(size_t)A.Col[k]] == s);
+      while (cur[(size_t)r] + c < dptr[(size_t)r + 1] && seg_of[(size_t)A.Col[dk[(size_t)(cur[(size_t)r] + c)]]] == s) c++;
       scount[(size_t)r] = c;
     }
     int64_t step = 0;
@@ -672,8 +684,10 @@ Bundle* build_lav(const Crs<T>& A, int64_t L, double Tthr, int64_t seglen) {
       chunk_full[(size_t)(s * chunk_count + c)] = (int)(step + minc);
       std::vector<std::vector<std::pair<uint32_t, T>>> ent(rows.size());
       for (size_t i = 0; i < rows.size(); ++i)
-        for (int64_t k = A.Rst[rows[i]]; k < A.Rst[rows[i] + 1]; ++k)
-          if (seg_of[(size_t)A.Col[k]] == s) ent[i].emplace_back((uint32_t)A.Col[k], A.Val[k]);
+        for (int64_t q = 0; q < scount[rows[i]]; ++q) {
+          const int k = dk[(size_t)(cur[rows[i]] + q)];
+          ent[i].emplace_back((uint32_t)A.Col[k], A.Val[k]);
+        }
       for (int64_t q = 0; q < maxc; ++q) {
         uint16_t active = 0;
         for (int64_t i = 0; i < L; ++i) {
@@ -686,6 +700,7 @@ Bundle* build_lav(const Crs<T>& A, int64_t L, double Tthr, int64_t seglen) {
       }
       step += maxc;
     }
+    for (int64_t r = 0; r < m; ++r) cur[(size_t)r] += scount[(size_t)r];
     chunk_offsets[(size_t)((chunk_count + 1) * s + chunk_count)] = (int)step;
     segment_ptr[(size_t)s + 1] = segment_ptr[(size_t)s] + (uint64_t)step;
   }
@@ -790,16 +805,15 @@ Bundle* build_vnec(const Crs<T>& A, int64_t NT, int64_t force) {
   }
   // per-thread compaction (merge-path ranges)
   std::vector<int> ecr((size_t)nnz, 0), nec((size_t)NT, 0), ux_ptr((size_t)NT + 1, 0), ux;
-  std::vector<int> mark((size_t)n, -1);
+  std::vector<int> mark((size_t)n, -1), rank((size_t)n, 0);  // rank: column -> compacted index
   for (int64_t t = 0; t < NT; ++t) {
     int64_t y0 = tcs[(size_t)(2 * t + 1)], y1 = tce[(size_t)(2 * t + 1)];
     std::vector<int> used;
     for (int64_t j = y0; j < y1; ++j)
       if (mark[(size_t)A.Col[j]] != (int)t) { mark[(size_t)A.Col[j]] = (int)t; used.push_back(A.Col[j]); }
     std::sort(used.begin(), used.end());
-    std::map<int, int> rank;
-    for (size_t k = 0; k < used.size(); ++k) rank[used[k]] = (int)k;
-    for (int64_t j = y0; j < y1; ++j) ecr[(size_t)j] = rank[A.Col[j]];
+    for (size_t k = 0; k < used.size(); ++k) rank[(size_t)used[k]] = (int)k;
+    for (int64_t j = y0; j < y1; ++j) ecr[(size_t)j] = rank[(size_t)A.Col[j]];
     nec[(size_t)t] = (int)used.size();
     ux.insert(ux.end(), used.begin(), used.end());
     ux_ptr[(size_t)t + 1] = (int)ux.size();
@@ -876,8 +890,7 @@ Bundle* build_vnec(const Crs<T>& A, int64_t NT, int64_t force) {
         for (int64_t k = A.Rst[r]; k < A.Rst[r + 1]; ++k)
           if (mark[(size_t)A.Col[k]] != (int)(NT + t)) { mark[(size_t)A.Col[k]] = (int)(NT + t); used.push_back(A.Col[k]); }
       std::sort(used.begin(), used.end());
-      std::map<int, int> rank;
-      for (size_t k = 0; k < used.size(); ++k) rank[used[k]] = (int)k;
+      for (size_t k = 0; k < used.size(); ++k) rank[(size_t)used[k]] = (int)k;
       nec_s[(size_t)t] = (int)used.size();
       uxs.insert(uxs.end(), used.begin(), used.end());
       uxs_ptr[(size_t)t + 1] = (int)uxs.size();
@@ -902,7 +915,7 @@ Bundle* build_vnec(const Crs<T>& A, int64_t NT, int64_t force) {
           rbeg.push_back(base);
           rend.push_back(base + (int)rl);
           for (int64_t c = 0; c < A.Rst[r + 1] - A.Rst[r]; ++c) {
-            rcol[(size_t)(base + c * nL + k)] = rank[A.Col[A.Rst[r] + c]];
+            rcol[(size_t)(base + c * nL + k)] = rank[(size_t)A.Col[A.Rst[r] + c]];
             rval[(size_t)(base + c * nL + k)] = A.Val[A.Rst[r] + c];
           }
         }
@@ -910,7 +923,7 @@ Bundle* build_vnec(const Crs<T>& A, int64_t NT, int64_t force) {
       for (int r : inrow) {
         tasks.push_back(r);
         rbeg.push_back((int)rcol.size());
-        for (int64_t k = A.Rst[r]; k < A.Rst[r + 1]; ++k) { rcol.push_back(rank[A.Col[k]]); rval.push_back(A.Val[k]); }
+        for (int64_t k = A.Rst[r]; k < A.Rst[r + 1]; ++k) { rcol.push_back(rank[(size_t)A.Col[k]]); rval.push_back(A.Val[k]); }
         rend.push_back((int)rcol.size());
       }
       tend[(size_t)t] = (int)tasks.size();
