@@ -451,6 +451,16 @@ int rvvla_csr5_spmv_f32(const rvvla_csr5* A, float alpha, const float* x, float 
  * lane sums fp32 two-sum, cross-lane and cross-tile merges fp64. */
 int rvvla_csr5_spmv_mixed(const rvvla_csr5* A, int val_type, float alpha, const float* x,
                           float beta, float* y, void* stream);
+/* rvvla_csr5_spmv_f64 without any device allocation (no counterpart in the
+ * reference): the per-warp calibrator lives in a static device array of
+ * 8192 slots (96 KB), enough for every launch on a B200; a matrix whose
+ * launch needs more returns RVVLA_ERR_TOO_LARGE.  The first call on each
+ * device resolves that array's address (and may load the module): make it
+ * before any stream capture.  Calls overlapping in time on one device share
+ * the array and race: serialise them.  Always runs the register-staged
+ * kernel. */
+int rvvla_csr5_spmv_f64_noalloc(const rvvla_csr5* A, double alpha, const double* x, double beta,
+                                double* y, void* stream);
 
 /* ------------------------------------------------------------ workloads
  * Seeded synthetic matrices on the host (OpenMP), written into caller

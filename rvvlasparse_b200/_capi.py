@@ -207,6 +207,7 @@ def load():
     _proto(lib, "rvvla_csr5_spmv_f64", cint, P(rvvla_csr5), dbl, vp, dbl, vp, vp)
     _proto(lib, "rvvla_csr5_spmv_f32", cint, P(rvvla_csr5), flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_csr5_spmv_mixed", cint, P(rvvla_csr5), cint, flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_csr5_spmv_f64_noalloc", cint, P(rvvla_csr5), dbl, vp, dbl, vp, vp)
     # workloads
     _proto(lib, "rvvla_gen_laplace2d", i64, i64, vp, vp, vp)
     _proto(lib, "rvvla_gen_stencil27", i64, i64, u64, vp, vp, vp)

@@ -625,7 +625,7 @@ int csr5_validate(const rvvla_csr5* A, const void* x, const void* y) {
 
 template <class V, class X, class Ac, class CT>
 int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaStream_t st, CT* cal_buf,
-                   int* cal_row_buf, int64_t cal_cap) {
+                   int* cal_row_buf, int64_t cal_cap, int* status_word, bool regs_only) {
   int rc = csr5_validate(A, x, y);
   if (rc) return rc;
   if (A->m == 0) return RVVLA_OK;
@@ -654,13 +654,13 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
     const uint32_t* eo_ptr = A->tile_empty_offset_pointer;
     const uint32_t* eo = A->tile_empty_offset;
     const V* vals = (const V*)A->csr_value;
-    int* status = device_status_word();
+    int* status = status_word ? status_word : device_status_word();
     if (!status) return fail(RVVLA_ERR_CUDA, "csr5: no device status word");
     // bulk copies need 16-byte aligned sources; other layouts take the
     // register-only kernel
     const bool aligned = ((uintptr_t)A->csr_value % 16 == 0) && ((uintptr_t)A->csr_column_index % 16 == 0) &&
                          ((uintptr_t)A->tile_descriptor % 16 == 0);
-    const bool use_regs = csr5_register_variant();
+    const bool use_regs = regs_only || csr5_register_variant();
     switch (aligned ? A->sigma : -1) {
 #define CSR5_CASE(S)                                                                                         \
   case S: {                                                                                                  \
@@ -791,8 +791,8 @@ int csr5_build_impl(const rvvla_crs* src, int vb, int omega, int sigma, rvvla_cs
 
 template <class V, class X, class Ac, class CT>
 int csr5_spmv_dispatch(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaStream_t st, CT* cal,
-                       int* cal_row, int64_t cap) {
-  return csr5_spmv_impl<V, X, Ac, CT>(A, alpha, x, beta, y, st, cal, cal_row, cap);
+                       int* cal_row, int64_t cap, int* status_word, bool regs_only) {
+  return csr5_spmv_impl<V, X, Ac, CT>(A, alpha, x, beta, y, st, cal, cal_row, cap, status_word, regs_only);
 }
 
 // Calibrator entries the SpMV of this matrix needs (one per warp).
@@ -805,14 +805,16 @@ int64_t csr5_calibrator_len(const rvvla_csr5* A) {
 }
 
 template int csr5_spmv_dispatch<double, double, double, double>(const rvvla_csr5*, double, const double*, double,
-                                                                double*, cudaStream_t, double*, int*, int64_t);
+                                                                double*, cudaStream_t, double*, int*, int64_t,
+                                                                int*, bool);
 template int csr5_spmv_dispatch<float, float, float, float>(const rvvla_csr5*, float, const float*, float, float*,
-                                                            cudaStream_t, float*, int*, int64_t);
+                                                            cudaStream_t, float*, int*, int64_t, int*, bool);
 template int csr5_spmv_dispatch<float, float, CompF32, double>(const rvvla_csr5*, float, const float*, float,
-                                                               float*, cudaStream_t, double*, int*, int64_t);
+                                                               float*, cudaStream_t, double*, int*, int64_t, int*,
+                                                               bool);
 template int csr5_spmv_dispatch<__nv_bfloat16, float, CompF32, double>(const rvvla_csr5*, float, const float*,
                                                                        float, float*, cudaStream_t, double*, int*,
-                                                                       int64_t);
+                                                                       int64_t, int*, bool);
 
 }  // namespace rvvla
 
@@ -845,22 +847,22 @@ void rvvla_csr5_free(rvvla_csr5_owned* h) {
 
 int rvvla_csr5_spmv_f64(const rvvla_csr5* A, double alpha, const double* x, double beta, double* y, void* stream) {
   return csr5_spmv_dispatch<double, double, double, double>(A, alpha, x, beta, y, as_stream(stream), nullptr,
-                                                            nullptr, 0);
+                                                            nullptr, 0, nullptr, false);
 }
 
 int rvvla_csr5_spmv_f32(const rvvla_csr5* A, float alpha, const float* x, float beta, float* y, void* stream) {
   return csr5_spmv_dispatch<float, float, float, float>(A, alpha, x, beta, y, as_stream(stream), nullptr, nullptr,
-                                                        0);
+                                                        0, nullptr, false);
 }
 
 int rvvla_csr5_spmv_mixed(const rvvla_csr5* A, int val_type, float alpha, const float* x, float beta, float* y,
                           void* stream) {
   if (val_type == RVVLA_F32)
     return csr5_spmv_dispatch<float, float, CompF32, double>(A, alpha, x, beta, y, as_stream(stream), nullptr,
-                                                             nullptr, 0);
+                                                             nullptr, 0, nullptr, false);
   if (val_type == RVVLA_BF16)
     return csr5_spmv_dispatch<__nv_bfloat16, float, CompF32, double>(A, alpha, x, beta, y, as_stream(stream),
-                                                                     nullptr, nullptr, 0);
+                                                                     nullptr, nullptr, 0, nullptr, false);
   return fail(RVVLA_ERR_INVALID_ARG, "csr5_spmv_mixed: val_type must be RVVLA_F32 or RVVLA_BF16");
 }
 
