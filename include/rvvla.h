@@ -76,6 +76,11 @@ uint64_t rvvla_kernel_launch_count(void);
  * stream synchronisation; for callers that manage memory themselves (the
  * builders hand back library-allocated arrays). */
 int rvvla_memcpy(void* dst, const void* src, size_t bytes, void* stream);
+/* cudaMalloc / cudaFree on the current device, for host code (the C++
+ * drop-in) that keeps device copies without linking the CUDA runtime itself.
+ * rvvla_malloc of 0 bytes yields NULL. */
+int rvvla_malloc(void** ptr, size_t bytes);
+int rvvla_free(void* ptr);
 /* Synchronises `stream`, then reads and clears the device status word that
  * kernels with bounded waits (the bulk-copy pipelines) set when a wait
  * expires.  *code = 0 and RVVLA_OK when no wait expired since the last call;
@@ -461,6 +466,44 @@ int rvvla_csr5_spmv_mixed(const rvvla_csr5* A, int val_type, float alpha, const 
  * kernel. */
 int rvvla_csr5_spmv_f64_noalloc(const rvvla_csr5* A, double alpha, const double* x, double beta,
                                 double* y, void* stream);
+
+/* ------------------------------------------------------------ adjoint
+ * No reference counterpart (the reference declares SPARSE_OPERATION_TRANSPOSE
+ * in include/types.h:24-27 and ignores it).  For y = alpha*A(v)*x with a fixed
+ * pattern: dx = A^T g through a transposed CRS built on the GPU, and
+ * dv[k] = g[row(k)] * x[Col[k]] on A's pattern (SDDMM). */
+typedef struct rvvla_transpose {
+  rvvla_crs AT;         /* A^T: n x m CRS, with its analysis plan */
+  const int32_t* perm;  /* perm[k] = index in A of A^T's k-th nonzero */
+  int32_t val_bytes;    /* element size of AT.Val: 8, 4 or 2 */
+} rvvla_transpose;
+
+typedef struct rvvla_transpose_owned {
+  rvvla_transpose h;
+  int32_t *Rst, *Col, *perm, *plan;
+  void* Val;
+} rvvla_transpose_owned;
+
+/* Builds A^T (entries of a column in ascending row order) and the
+ * permutation; copies A's values when A->Val is not NULL.  Synchronises
+ * `stream`. */
+int rvvla_csr_transpose(const rvvla_crs* A, int val_bytes, rvvla_transpose_owned* out,
+                        void* stream);
+void rvvla_csr_transpose_free(rvvla_transpose_owned* h);
+/* ValT[k] = Val[perm[k]]: refreshes A^T's values after A's values changed. */
+int rvvla_csr_transpose_values(const rvvla_transpose* T, const void* Val, void* ValT,
+                               void* stream);
+/* dx = alpha * A^T g + beta * dx (the CRS kernels on A^T; beta = 0 does not
+ * read dx). */
+int rvvla_spmv_adjoint_x_f64(const rvvla_transpose* T, double alpha, const double* g,
+                             double beta, double* dx, void* stream);
+int rvvla_spmv_adjoint_x_f32(const rvvla_transpose* T, float alpha, const float* g,
+                             float beta, float* dx, void* stream);
+/* dvalues[k] = g[row(k)] * x[Col[k]] for every nonzero k of A. */
+int rvvla_sddmm_values_f64(const rvvla_crs* A, const double* g, const double* x, double* dvalues,
+                           void* stream);
+int rvvla_sddmm_values_f32(const rvvla_crs* A, const float* g, const float* x, float* dvalues,
+                           void* stream);
 
 /* ------------------------------------------------------------ workloads
  * Seeded synthetic matrices on the host (OpenMP), written into caller

@@ -60,6 +60,14 @@ VNEC_ARRAYS = ("ptr", "indices", "val", "thread_coord_start", "thread_coord_end"
                "task_end", "spvv_len", "row_begin", "row_end", "reorder_col", "reorder_nnz")
 
 
+class rvvla_transpose(C.Structure):
+    _fields_ = [("AT", rvvla_crs), ("perm", vp), ("val_bytes", i32)]
+
+
+class rvvla_transpose_owned(C.Structure):
+    _fields_ = [("h", rvvla_transpose), ("Rst", vp), ("Col", vp), ("perm", vp), ("plan", vp), ("Val", vp)]
+
+
 class rvvla_lav(C.Structure):
     _fields_ = [("SIMD_Lanes", i64), ("m", i64), ("n", i64), ("nz", i64), ("segment_count", i64),
                 ("chunk_count", i64), ("segment_len", i64), ("n_steps", i64), ("T", dbl), ("chunk_offsets", vp),
@@ -162,6 +170,8 @@ def load():
     _proto(lib, "rvvla_device_info", cint, P(cint), P(cint), P(cint))
     _proto(lib, "rvvla_kernel_launch_count", u64)
     _proto(lib, "rvvla_memcpy", cint, vp, vp, C.c_size_t, vp)
+    _proto(lib, "rvvla_malloc", cint, P(vp), C.c_size_t)
+    _proto(lib, "rvvla_free", cint, vp)
     _proto(lib, "rvvla_device_status", cint, P(cint), vp)
     # CRS
     _proto(lib, "rvvla_crs_plan_len", i64, i64, i64, cint)
@@ -208,6 +218,14 @@ def load():
     _proto(lib, "rvvla_csr5_spmv_f32", cint, P(rvvla_csr5), flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_csr5_spmv_mixed", cint, P(rvvla_csr5), cint, flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_csr5_spmv_f64_noalloc", cint, P(rvvla_csr5), dbl, vp, dbl, vp, vp)
+    # adjoint
+    _proto(lib, "rvvla_csr_transpose", cint, P(rvvla_crs), cint, P(rvvla_transpose_owned), vp)
+    _proto(lib, "rvvla_csr_transpose_free", None, P(rvvla_transpose_owned))
+    _proto(lib, "rvvla_csr_transpose_values", cint, P(rvvla_transpose), vp, vp, vp)
+    _proto(lib, "rvvla_spmv_adjoint_x_f64", cint, P(rvvla_transpose), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_spmv_adjoint_x_f32", cint, P(rvvla_transpose), flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_sddmm_values_f64", cint, P(rvvla_crs), vp, vp, vp, vp)
+    _proto(lib, "rvvla_sddmm_values_f32", cint, P(rvvla_crs), vp, vp, vp, vp)
     # workloads
     _proto(lib, "rvvla_gen_laplace2d", i64, i64, vp, vp, vp)
     _proto(lib, "rvvla_gen_stencil27", i64, i64, u64, vp, vp, vp)

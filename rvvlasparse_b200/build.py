@@ -2,11 +2,12 @@
 
 Every ``csrc/*.cu`` file is compiled by nvcc for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``) in parallel, ``csrc/*.cpp``
-(host code: workload generators, the C++ drop-in layer) with the same nvcc
-host compiler, and the objects are linked into one shared library with the
-CUDA runtime linked statically.  Objects are rebuilt only when a source or
-header is newer.  The drop-in C++ test program under ``dropin/`` is built by
-``build_dropin_test``.
+(host code: workload generators, the VNEC/LAV host builders) with the same
+nvcc host compiler, and the objects are linked into one shared library with
+the CUDA runtime linked statically.  Objects are rebuilt only when a source or
+header is newer.  ``build_dropin`` then compiles the C++ drop-in
+(``dropin/dropin.cpp`` -> ``lib/librvvla_dropin.so``, the reference's C++ API
+over the C ABI) and its test program (``_build/test_dropin``).
 
 Usage: ``python -m rvvlasparse_b200.build`` (or ``__graft_entry__.build()``).
 """
@@ -103,6 +104,40 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     return LIB
 
 
+DROPIN = os.path.join(PKG, "dropin")
+DROPIN_LIB = os.path.join(LIB_DIR, "librvvla_dropin.so")
+DROPIN_TEST = os.path.join(PKG, "_build", "test_dropin")
+
+
+def build_dropin(verbose: bool = False) -> str:
+    """Compile the C++ drop-in library and its test program (host code only,
+    linked against ``librvvla_b200.so``); returns the library path."""
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+    inc = ["-I" + INCLUDE, "-I" + os.path.join(DROPIN, "include")]
+    hdrs = glob.glob(os.path.join(DROPIN, "include", "*.h")) + [os.path.join(INCLUDE, "rvvla.h")]
+    steps = [
+        (DROPIN_LIB, [os.path.join(DROPIN, "dropin.cpp")],
+         [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall"] + inc + [os.path.join(DROPIN, "dropin.cpp"),
+          "-L" + LIB_DIR, "-lrvvla_b200", "-Wl,-rpath,$ORIGIN", "-o"]),
+        (DROPIN_TEST, [os.path.join(DROPIN, "test_dropin.cpp"), DROPIN_LIB],
+         [cxx, "-std=c++17", "-O2", "-Wall"] + inc + [os.path.join(DROPIN, "test_dropin.cpp"), "-L" + LIB_DIR,
+          "-lrvvla_dropin", "-lrvvla_b200", "-Wl,-rpath,$ORIGIN/../lib", "-o"]),
+    ]
+    os.makedirs(os.path.dirname(DROPIN_TEST), exist_ok=True)
+    for target, srcs, cmd in steps:
+        if not _stale(target, srcs + hdrs + [LIB]):
+            continue
+        tmp = target + ".tmp"
+        cmd = cmd + [tmp]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"drop-in build failed ({os.path.basename(target)}):\n{res.stdout}\n{res.stderr}")
+        os.replace(tmp, target)
+    return DROPIN_LIB
+
+
 def ptxas_report(src: str) -> str:
     """Register / spill / shared-memory report (-Xptxas -v) for one source."""
     cmd = [_nvcc()] + _host_cxx() + _common_flags() + ARCH + ["-Xptxas", "-v", "-c", src, "-o", os.devnull]
@@ -112,4 +147,5 @@ def ptxas_report(src: str) -> str:
 
 if __name__ == "__main__":
     path = build(verbose="-v" in sys.argv)
+    build_dropin(verbose="-v" in sys.argv)
     print(path)

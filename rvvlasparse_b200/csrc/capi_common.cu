@@ -111,6 +111,19 @@ int rvvla_device_status(int* code, void* stream) {
   return *code ? RVVLA_ERR_TIMEOUT : RVVLA_OK;
 }
 
+int rvvla_malloc(void** ptr, size_t bytes) {
+  if (!ptr) return rvvla::fail(RVVLA_ERR_INVALID_ARG, "rvvla_malloc: null pointer");
+  *ptr = nullptr;
+  if (bytes == 0) return RVVLA_OK;
+  RVVLA_CUDA(cudaMalloc(ptr, bytes));
+  return RVVLA_OK;
+}
+
+int rvvla_free(void* ptr) {
+  if (ptr) RVVLA_CUDA(cudaFree(ptr));
+  return RVVLA_OK;
+}
+
 int rvvla_memcpy(void* dst, const void* src, size_t bytes, void* stream) {
   if (bytes == 0) return RVVLA_OK;
   if (!dst || !src) return rvvla::fail(RVVLA_ERR_INVALID_ARG, "rvvla_memcpy: null pointer");

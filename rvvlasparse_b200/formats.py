@@ -618,7 +618,9 @@ def _vec_type(mat, mixed: bool) -> torch.dtype:
 
 def _spmv(op, alpha, mat, descr, b, beta, y, mixed: bool, stage=SPARSE_MATRIX_MV_ALL_STAGES):
     status = sparse_matrix_status()
-    if int(op) != int(SPARSE_OPERATION_NON_TRANSPOSE):
+    transpose = int(op) == int(SPARSE_OPERATION_TRANSPOSE)
+    if transpose and (mixed or not isinstance(mat, spMtxCRS) or mat.dtype not in (torch.float64, torch.float32)):
+        # A^T b exists for CRS (through the adjoint's transposed layout) only
         status.code = _capi.RVVLA_ERR_UNSUPPORTED
         return status
     vt = _vec_type(mat, mixed)
@@ -631,11 +633,51 @@ def _spmv(op, alpha, mat, descr, b, beta, y, mixed: bool, stage=SPARSE_MATRIX_MV
     if b.dtype != vt or y.dtype != vt or not b.is_cuda or not y.is_cuda:
         status.code = _capi.RVVLA_ERR_INVALID_ARG
         return status
-    status.code = _call_spmv(mat, alpha, b, beta, y, mixed) if stage == SPARSE_MATRIX_MV_ALL_STAGES \
-        else _call_stage(mat, alpha, b, beta, y, stage)
+    if transpose:
+        status.code = _call_transpose(mat, alpha, b, beta, y) if stage in (SPARSE_MATRIX_MV_ALL_STAGES,
+                                                                          SPARSE_MATRIX_MV_MULT) else 0
+    else:
+        status.code = _call_spmv(mat, alpha, b, beta, y, mixed) if stage == SPARSE_MATRIX_MV_ALL_STAGES \
+            else _call_stage(mat, alpha, b, beta, y, stage)
     if host_y is not None and status.code == 0:
         host_y[...] = y.cpu().numpy()
     return status
+
+
+def _call_transpose(mat: "spMtxCRS", alpha, b, beta, y) -> int:
+    """y <- alpha*A^T*b + beta*y: the transposed CRS is built on the GPU once
+    per matrix (rvvla_csr_transpose) and multiplied by the CRS kernels."""
+    if b.numel() < mat.m or y.numel() < mat.n:
+        return _capi.RVVLA_ERR_INVALID_ARG
+    lib = load()
+    key = (mat.Rst.data_ptr(), mat.Col.data_ptr(), mat.Val.dtype)
+    tr = getattr(mat, "_transpose", None)
+    if tr is None or tr[1] != key:
+        owned = _capi.rvvla_transpose_owned()
+        st = lib.rvvla_csr_transpose(C.byref(mat.desc()), mat.Val.element_size(), C.byref(owned), _stream())
+        if st != 0:
+            return st
+        tr = (_TransposeHandle(owned), key)
+        mat._transpose = tr
+    else:  # same pattern: refresh the values (they may have changed in place)
+        st = lib.rvvla_csr_transpose_values(C.byref(tr[0].owned.h), _ptr(mat.Val), tr[0].owned.Val, _stream())
+        if st != 0:
+            return st
+    fn = lib.rvvla_spmv_adjoint_x_f64 if mat.dtype == torch.float64 else lib.rvvla_spmv_adjoint_x_f32
+    return fn(C.byref(tr[0].owned.h), float(alpha), _ptr(b), float(beta), _ptr(y), _stream())
+
+
+class _TransposeHandle:
+    """Owns a library-built transposed CRS (freed with the matrix)."""
+
+    def __init__(self, owned):
+        self.owned = owned
+
+    def __del__(self):
+        try:
+            load().rvvla_csr_transpose_free(C.byref(self.owned))
+        except Exception:
+            pass
 
 
 def _call_stage(mat, alpha, b, beta, y, stage):

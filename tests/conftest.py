@@ -19,6 +19,7 @@ def _built_libraries():
     from rvvlasparse_b200 import build
 
     build.build()
+    build.build_dropin()
     oracle.build(ref=True)
     yield
 

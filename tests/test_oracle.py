@@ -117,3 +117,22 @@ def test_merge_path_split_matches_definition():
         assert all(ends[i] <= y for i in range(x))
         if x < len(ends) and y > 0:
             assert not (ends[x] <= y - 1)
+
+
+def test_transpose_and_sddmm_definitions(g):
+    """The oracle's transpose (with permutation) and SDDMM against scipy and
+    the definitions (they anchor the GPU adjoint tests)."""
+    import scipy.sparse as sp
+
+    m, n = g["m"], g["n"]
+    A = O.crs(m, n, g["Rst"], g["Col"], g["Val"])
+    t = O.transpose(A)
+    S = sp.csr_matrix((g["Val"], g["Col"], g["Rst"]), shape=(m, n)).T.tocsr()
+    S.sort_indices()
+    assert np.array_equal(t["Rst"], S.indptr) and np.array_equal(t["Col"], S.indices)
+    assert np.array_equal(t["Val"], S.data)
+    assert np.array_equal(t["Val"], g["Val"][t["perm"]])
+    rows = np.repeat(np.arange(m), np.diff(g["Rst"]))
+    gv = np.linspace(-1, 1, m)
+    dv = O.sddmm(A, gv, g["x"])
+    assert np.array_equal(dv, gv[rows] * g["x"].astype(np.float64)[g["Col"]])
