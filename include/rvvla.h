@@ -505,6 +505,57 @@ int rvvla_sddmm_values_f64(const rvvla_crs* A, const double* g, const double* x,
 int rvvla_sddmm_values_f32(const rvvla_crs* A, const float* g, const float* x, float* dvalues,
                            void* stream);
 
+/* ------------------------------------------------------------ batched
+ * No reference counterpart.  Many independent matrices, each with k right-
+ * hand sides, in one persistent launch: Y_i = alpha * A_i X_i + beta * Y_i.
+ * X_i is n_i x k and Y_i is m_i x k, row-major, packed matrix after matrix
+ * (matrix i starts at x_off[i] / y_off[i] elements). */
+typedef struct rvvla_batch {
+  int64_t count, k, x_len, y_len, ntiles;
+  int32_t val_bytes, grid, block;
+  const void* mats;   /* device table, one entry per matrix */
+  const void* tiles;  /* device work list */
+} rvvla_batch;
+
+typedef struct rvvla_batch_owned {
+  rvvla_batch h;
+  void* mats;
+  void* tiles;
+  int64_t* x_off;          /* host, count + 1 entries */
+  int64_t* y_off;          /* host, count + 1 entries */
+  rvvla_sell_owned* sell;  /* host, the SELL copies of mode-1 matrices */
+  int64_t nmats;
+} rvvla_batch_owned;
+
+/* Plans a batch of CRS matrices (device arrays, which must stay alive):
+ * val_bytes 4 or 8; k in {1, 4, 8, 32}; mode[i] 0 = CSR (param[i] = threads
+ * per row for k = 1, a power of two <= 32, 0 = by average row length) or
+ * 1 = SELL-C-sigma with C = 32 built on the GPU (param[i] = sigma, 0 = 256);
+ * mode/param may be NULL (all CSR, default threads per row).  Synchronises
+ * `stream`. */
+int rvvla_batched_plan(const rvvla_crs* mats, int64_t count, int val_bytes, int k, const int32_t* mode,
+                       const int32_t* param, rvvla_batch_owned* out, void* stream);
+void rvvla_batched_free(rvvla_batch_owned* b);
+/* One persistent launch over all matrices. */
+int rvvla_batched_spmv_f64(const rvvla_batch* B, double alpha, const double* X, double beta, double* Y,
+                           void* stream);
+int rvvla_batched_spmv_f32(const rvvla_batch* B, float alpha, const float* X, float beta, float* Y,
+                           void* stream);
+/* Captures that launch (fixed alpha, X, beta, Y) into a CUDA graph on a
+ * non-default `stream` and instantiates it; *graph is an opaque handle. */
+int rvvla_batched_graph(const rvvla_batch* B, double alpha, const void* X, double beta, void* Y,
+                        void* stream, void** graph);
+int rvvla_batched_graph_launch(void* graph, void* stream);
+void rvvla_batched_graph_free(void* graph);
+/* Autotuner: groups the matrices by average row length (powers of two),
+ * times every candidate configuration on each group with CUDA events (CSR
+ * with 1..32 threads per row for k = 1 or k lanes per row otherwise;
+ * SELL-C-sigma with sigma 32 or 256) and writes the fastest per matrix into
+ * mode[] / param[] (count entries each), ready for rvvla_batched_plan.
+ * *tuned_ms (may be NULL) receives the sum of the groups' best times. */
+int rvvla_batched_autotune(const rvvla_crs* mats, int64_t count, int val_bytes, int k, int32_t* mode,
+                           int32_t* param, double* tuned_ms, void* stream);
+
 /* ------------------------------------------------------------ workloads
  * Seeded synthetic matrices on the host (OpenMP), written into caller
  * buffers in two calls: first with NULL arrays to learn nz, then with

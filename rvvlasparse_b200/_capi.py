@@ -68,6 +68,16 @@ class rvvla_transpose_owned(C.Structure):
     _fields_ = [("h", rvvla_transpose), ("Rst", vp), ("Col", vp), ("perm", vp), ("plan", vp), ("Val", vp)]
 
 
+class rvvla_batch(C.Structure):
+    _fields_ = [("count", i64), ("k", i64), ("x_len", i64), ("y_len", i64), ("ntiles", i64), ("val_bytes", i32),
+                ("grid", i32), ("block", i32), ("mats", vp), ("tiles", vp)]
+
+
+class rvvla_batch_owned(C.Structure):
+    _fields_ = [("h", rvvla_batch), ("mats", vp), ("tiles", vp), ("x_off", C.POINTER(i64)),
+                ("y_off", C.POINTER(i64)), ("sell", vp), ("nmats", i64)]
+
+
 class rvvla_lav(C.Structure):
     _fields_ = [("SIMD_Lanes", i64), ("m", i64), ("n", i64), ("nz", i64), ("segment_count", i64),
                 ("chunk_count", i64), ("segment_len", i64), ("n_steps", i64), ("T", dbl), ("chunk_offsets", vp),
@@ -226,6 +236,15 @@ def load():
     _proto(lib, "rvvla_spmv_adjoint_x_f32", cint, P(rvvla_transpose), flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_sddmm_values_f64", cint, P(rvvla_crs), vp, vp, vp, vp)
     _proto(lib, "rvvla_sddmm_values_f32", cint, P(rvvla_crs), vp, vp, vp, vp)
+    # batched
+    _proto(lib, "rvvla_batched_plan", cint, P(rvvla_crs), i64, cint, cint, vp, vp, P(rvvla_batch_owned), vp)
+    _proto(lib, "rvvla_batched_free", None, P(rvvla_batch_owned))
+    _proto(lib, "rvvla_batched_spmv_f64", cint, P(rvvla_batch), dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_batched_spmv_f32", cint, P(rvvla_batch), flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_batched_graph", cint, P(rvvla_batch), dbl, vp, dbl, vp, vp, P(vp))
+    _proto(lib, "rvvla_batched_graph_launch", cint, vp, vp)
+    _proto(lib, "rvvla_batched_graph_free", None, vp)
+    _proto(lib, "rvvla_batched_autotune", cint, P(rvvla_crs), i64, cint, cint, vp, vp, P(dbl), vp)
     # workloads
     _proto(lib, "rvvla_gen_laplace2d", i64, i64, vp, vp, vp)
     _proto(lib, "rvvla_gen_stencil27", i64, i64, u64, vp, vp, vp)

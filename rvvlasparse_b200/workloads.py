@@ -63,3 +63,15 @@ def vector(n: int, seed: int = 0, normal: bool = False, lo: float = -1.0, hi: fl
     out = np.empty(n, dtype=np.float64)
     lib.rvvla_gen_vector(n, seed, 1 if normal else 0, lo, hi, out.ctypes.data)
     return out
+
+
+def batch(count: int = 1024, n_lo: int = 1024, n_hi: int = 65536, avg_lo: float = 4.0, avg_hi: float = 64.0,
+          seed: int = 7):
+    """The batched workload: ``count`` square matrices, n log-uniform in
+    [n_lo, n_hi], average nonzeros per row uniform in [avg_lo, avg_hi], Poisson
+    row lengths, uniform random columns, values uniform in [-1, 1]."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), count)).astype(np.int64)
+    avgs = rng.uniform(avg_lo, avg_hi, count)
+    return [random_rows(int(n), int(n), "poisson", float(a), "uniform", seed=seed * 100003 + i)
+            for i, (n, a) in enumerate(zip(ns, avgs))]
