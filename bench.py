@@ -71,7 +71,7 @@ class Case:
         import torch
 
         self.name, self.mat, self.prec, self.bytes, self.nnz = name, mat, prec, nbytes, nnz
-        vt = torch.float64 if prec == "f64" else torch.float32
+        vt = torch.float64 if prec == "f64" else torch.float32  # mixed forms: fp32 x and y
         self.vt = vt
         self.x = torch.empty(n, dtype=vt, device="cuda")
         self.y = torch.zeros(m, dtype=vt, device="cuda")
@@ -108,10 +108,14 @@ def sell_bytes(S, vb, xb):
 
 
 def lav_bytes(Lv, vb, xb):
-    # dense steps (values, columns, masks), out_order, chunk offsets (both),
-    # segment pointers, then the sparse part as CRS (with x and y)
+    # dense steps (values, columns, masks), chunk offsets (both), segment
+    # pointers, the row placement the kernel reads (one-pass kernel: the
+    # 1-byte slot->lane map and the row order; otherwise out_order), then the
+    # sparse part as CRS (with x and y)
     L, cc, ns = Lv.SIMD_Lanes, Lv.chunk_count, Lv.segment_count
-    dense = Lv.n_steps * L * (vb + 4) + Lv.n_steps * 2 + ns * cc * L * 4 + (2 * cc + 1) * ns * 4 + (ns + 1) * 8
+    fused = getattr(Lv, "lane_of_slot", None) is not None and L <= 32 and 32 % L == 0
+    place = ns * cc * L + Lv.m * 4 if fused else ns * cc * L * 4
+    dense = Lv.n_steps * L * (vb + 4) + Lv.n_steps * 2 + place + (2 * cc + 1) * ns * 4 + (ns + 1) * 8
     return dense + crs_bytes(Lv.m, Lv.n, Lv.sparse_part.nz, vb, xb)
 
 
@@ -136,6 +140,9 @@ MIXED = ("crs", "hcsr", "csr5", "sell")
 
 
 def build_cases(m, n, Rst, Col, Val, formats, precs):
+    """One Case per (format, precision).  Precisions: f64, f32, mixed (fp32
+    values, compensated fp32 sums, fp64 carry merges) and mixed_bf16 (the
+    same with bf16 values); the mixed forms exist for CRS, HCSR, CSR5, SELL."""
     import torch
 
     import rvvlasparse_b200 as R
@@ -145,55 +152,39 @@ def build_cases(m, n, Rst, Col, Val, formats, precs):
     A32 = A64.astype(torch.float32)
     nnz = A64.nz
     x64 = torch.as_tensor(np.random.default_rng(0).uniform(-1, 1, n)).cuda()
+    vbytes = {"f64": 8, "f32": 4, "mixed": 4, "mixed_bf16": 2}
+    spec = {
+        "crs": (None, {}, lambda M, vb, xb: crs_bytes(m, n, nnz, vb, xb)),
+        "hcsr": (R.spMtxHCSR, {}, lambda M, vb, xb: hcsr_bytes(M, vb, xb)),
+        "csr5": (R.spMtxCSR5, dict(omega=32, sigma=16),
+                 lambda M, vb, xb: csr5_bytes(m, n, nnz, M.p, M.omega, M.tile_desc_len, M.num_offsets, vb, xb)),
+        "sell": (R.spMtxSELL_C_Sigma, dict(C=32, sigma=256), sell_bytes),
+        # x stays in L2, so the GPU needs no column segments for cache
+        # blocking: one segment (segment_len = n) also avoids the padding that
+        # many short segments add (2.6x the dense part at the CPU default
+        # segment_len = 40000 on this matrix)
+        "lav": (R.spMtxLAV, dict(SIMD_Lanes=8, T=0.2, segment_len=max(n, 1)), lav_bytes),
+        "vnec": (R.spMtxVNEC, {}, vnec_bytes),
+        "vhcc": (R.spMtxVHCC, {}, vhcc_bytes),
+        "cvr": (R.spMtxCVR, {}, cvr_bytes)}
     for fmt in formats:
-        if fmt == "crs":
-            for p in precs:
-                if p == "f64":
-                    cases.append(Case("crs_f64", A64, "f64", crs_bytes(m, n, nnz, 8, 8), nnz, m, n))
-                elif p == "f32":
-                    cases.append(Case("crs_f32", A32, "f32", crs_bytes(m, n, nnz, 4, 4), nnz, m, n))
-                elif p == "mixed":
-                    cases.append(Case("crs_mixed", A32, "mixed", crs_bytes(m, n, nnz, 4, 4), nnz, m, n))
-        elif fmt == "hcsr":
-            H64 = R.spMtxHCSR()
-            R.convert(H64, A64, R.convertParams())
-            H32 = R.spMtxHCSR()
-            R.convert(H32, A32, R.convertParams())
-            for p in precs:
-                if p == "f64":
-                    cases.append(Case("hcsr_f64", H64, "f64", hcsr_bytes(H64, 8, 8), nnz, m, n))
-                elif p == "f32":
-                    cases.append(Case("hcsr_f32", H32, "f32", hcsr_bytes(H32, 4, 4), nnz, m, n))
-                elif p == "mixed":
-                    cases.append(Case("hcsr_mixed", H32, "mixed", hcsr_bytes(H32, 4, 4), nnz, m, n))
-        elif fmt == "csr5":
-            sig = {"f64": 16, "f32": 16, "mixed": 16}
-            for p in precs:
-                src = A64 if p == "f64" else A32
-                C5 = R.spMtxCSR5()
-                R.convert(C5, src, R.convertParams(omega=32, sigma=sig[p]))
-                vb = 8 if p == "f64" else 4
-                b = csr5_bytes(m, n, nnz, C5.p, C5.omega, C5.tile_desc_len, C5.num_offsets, vb, vb)
-                cases.append(Case(f"csr5_{p}", C5, p, b, nnz, m, n))
-        elif fmt in ("sell", "lav", "vnec", "vhcc", "cvr"):
-            cls, params, nbytes = {
-                "sell": (R.spMtxSELL_C_Sigma, dict(C=32, sigma=256), sell_bytes),
-                "lav": (R.spMtxLAV, dict(SIMD_Lanes=8, T=0.2, segment_len=40000), lav_bytes),
-                "vnec": (R.spMtxVNEC, {}, vnec_bytes),
-                "vhcc": (R.spMtxVHCC, {}, vhcc_bytes),
-                "cvr": (R.spMtxCVR, {}, cvr_bytes)}[fmt]
-            built = {}
-            for p in precs:
-                if p == "mixed" and fmt not in MIXED:
-                    continue
-                src = A64 if p == "f64" else A32
-                key = "f64" if p == "f64" else "f32"
-                if key not in built:
+        cls, params, nbytes = spec[fmt]
+        built = {}
+        for p in precs:
+            if p.startswith("mixed") and fmt not in MIXED:
+                continue
+            key = "f64" if p == "f64" else "f32"
+            if key not in built:
+                src = A64 if key == "f64" else A32
+                if cls is None:
+                    built[key] = src
+                else:
                     M = cls()
                     R.convert(M, src, R.convertParams(**params))
                     built[key] = M
-                vb = 8 if p == "f64" else 4
-                cases.append(Case(f"{fmt}_{p}", built[key], p, nbytes(built[key], vb, vb), nnz, m, n))
+            mat = built[key].astype(torch.bfloat16) if p == "mixed_bf16" else built[key]
+            vb, xb = vbytes[p], (8 if p == "f64" else 4)
+            cases.append(Case(f"{fmt}_{p}", mat, p, nbytes(mat, vb, xb), nnz, m, n))
     for c in cases:
         c.x.copy_(x64.to(c.vt))
     return cases
@@ -329,6 +320,13 @@ def run_gpu(args):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, m, n, Rst, Col, Val)
+    case_names = [c.name for c in cases]
+    case_precs = sorted({c.prec for c in cases})
+    forms = None
+    if world == 1 and not args.no_forms:
+        del cases
+        torch.cuda.empty_cache()
+        forms = run_forms(torch, pk)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -337,8 +335,8 @@ def run_gpu(args):
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": ",".join(sorted({c.prec for c in cases})), "data": "synthetic",
-        "config": {"workload": f"{args.workload} n={m} nnz={len(Col)}", "cases": [c.name for c in cases],
+        "vs_baseline": None, "dtype": ",".join(case_precs), "data": "synthetic",
+        "config": {"workload": f"{args.workload} n={m} nnz={len(Col)}", "cases": case_names,
                    "alpha": 1.0, "beta": 0.0, "parallelism": f"replicas{world}",
                    "l2": "matrix arrays larger than the 126 MB L2 (streamed from HBM every step); x L2-resident"},
         "per_format": per,
@@ -351,7 +349,181 @@ def run_gpu(args):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if forms is not None:
+        line["forms"] = forms
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- added forms
+def _time_ms(torch, fn, warmup=3, iters=20):
+    """Median CUDA-event time of fn() on the current stream.  The calls are
+    queued back to back (one synchronisation at the end), so each event pair
+    brackets the device work of one call, not the host time between calls."""
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(iters)]
+    torch.cuda.synchronize()
+    for e0, e1 in ev:
+        e0.record(st)
+        fn()
+        e1.record(st)
+    torch.cuda.synchronize()
+    return statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
+
+
+def form_precision(torch, pk):
+    """27-point stencil on a 128^3 grid (periodic, 56,623,104 nonzeros),
+    values 1 + 0.1 N(0,1), x U[-1,1]: plain fp64 against the mixed forms (fp32
+    or bf16 values, fp32 x/y, compensated fp32 row sums, fp64 carry merges)
+    for CSR5 and HCSR.  Errors are normwise and per-row against the
+    long-double oracle on the fp64 values ("vs_fp64") and on the stored
+    (rounded) values and x ("vs_stored": the accumulation error alone)."""
+    import oracle as O
+    import rvvlasparse_b200 as R
+    from rvvlasparse_b200 import workloads as W
+
+    m, n, Rst, Col, Val = W.stencil27(128, seed=3)
+    nnz = len(Col)
+    x = W.vector(n, 0)
+    z = np.zeros(m)
+    A = O.crs(m, n, Rst, Col, Val)
+    ref = O.crs_spmv_ld(A, 1.0, x, 0.0, z)
+    x32 = x.astype(np.float32)
+    ref32 = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val.astype(np.float32)), 1.0, x32.astype(np.float64), 0.0, z)
+    vbf = torch.as_tensor(Val).to(torch.bfloat16).to(torch.float64).numpy()
+    refbf = O.crs_spmv_ld(O.crs(m, n, Rst, Col, vbf), 1.0, x32.astype(np.float64), 0.0, z)
+
+    def errs(y, r):
+        nz = np.abs(r) > 0
+        rel = np.abs(y[nz] - r[nz]) / np.abs(r[nz])
+        return {"normwise": float(O.normwise_relerr(y, r)), "row_max": float(rel.max()),
+                "row_median": float(np.median(rel))}
+
+    A64 = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
+    A32 = A64.astype(torch.float32)
+    xd64 = torch.as_tensor(x).cuda()
+    xd32 = xd64.float()
+    out = {"workload": f"stencil27 128^3 n={m} nnz={nnz}", "formats": {}}
+    for fmt in ("csr5", "hcsr"):
+        cls, params = (R.spMtxCSR5, dict(omega=32, sigma=16)) if fmt == "csr5" else (R.spMtxHCSR, {})
+        M64, M32 = cls(), cls()
+        R.convert(M64, A64, R.convertParams(**params))
+        R.convert(M32, A32, R.convertParams(**params))
+        Mbf = M32.astype(torch.bfloat16)
+        res = {}
+        for name, M, mixed, xd, vb, xb, rr in (("f64", M64, False, xd64, 8, 8, None), ("mixed_f32", M32, True, xd32, 4, 4, ref32),
+                                                ("mixed_bf16", Mbf, True, xd32, 2, 4, refbf)):
+            y = torch.zeros(m, dtype=xd.dtype, device="cuda")
+            fn = R.sparse_mv_mixed if mixed else R.sparse_mv
+
+            def go():
+                st = fn(R.SPARSE_OPERATION_NON_TRANSPOSE, 1.0, M, R.sparse_matrix_descr(), xd, 0.0, y)
+                if st.code:
+                    raise RuntimeError(f"{fmt} {name}: {st.code}")
+
+            ms = _time_ms(torch, go)
+            yh = y.double().cpu().numpy()
+            b = (csr5_bytes(m, n, nnz, M.p, M.omega, M.tile_desc_len, M.num_offsets, vb, xb) if fmt == "csr5"
+                 else hcsr_bytes(M, vb, xb))
+            e = {"ms": round(ms, 4), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
+                 "frac_of_hbm": round(b / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4),
+                 "gnnz_per_s": round(nnz / (ms * 1e-3) / 1e9, 2), "vs_fp64": errs(yh, ref)}
+            if rr is not None:
+                e["vs_stored"] = errs(yh, rr)
+            res[name] = e
+        for name in ("mixed_f32", "mixed_bf16"):
+            res[name]["speedup_vs_f64"] = round(res["f64"]["ms"] / res[name]["ms"], 3)
+        out["formats"][fmt] = res
+    return out
+
+
+def form_batched(torch, pk):
+    """1,024 independent matrices (n log-uniform in [1024, 65536], average
+    nonzeros per row U[4, 64], Poisson rows, uniform columns, fp32 U[-1,1]),
+    k in {1, 4, 8, 32} right-hand sides; autotuned; one persistent launch per
+    product, replayed from a CUDA graph.  Bytes = 8*nnz + 4*(m+1) + 4*k*(n+m)
+    summed over the matrices."""
+    import oracle as O
+    import rvvlasparse_b200 as R
+    from rvvlasparse_b200 import batched as BT
+    from rvvlasparse_b200 import workloads as W
+
+    host = W.batch(1024, seed=7)
+    mats = [R.spMtxCRS.from_host(m, n, Rst, Col, Val.astype(np.float32), dtype=torch.float32)
+            for m, n, Rst, Col, Val in host]
+    snz = sum(len(h[2]) for h in host)
+    sm = sum(h[0] for h in host)
+    sn = sum(h[1] for h in host)
+    out = {"workload": f"1024 matrices, sum n = {sn}, sum nnz = {snz}, fp32", "k": {}}
+    s = torch.cuda.Stream()
+    for k in (1, 4, 8, 32):
+        with torch.cuda.stream(s):
+            B = BT.SpMVBatch(mats, k=k, tune=True)
+            X = torch.empty(B.x_len, dtype=torch.float32, device="cuda").uniform_(-1, 1)
+            Y = torch.zeros(B.y_len, dtype=torch.float32, device="cuda")
+            g = B.graph(1.0, X, 0.0, Y)
+            ms = _time_ms(torch, g.launch)
+            byts = 8 * snz + 4 * (sm + len(mats)) + 4 * k * (sn + sm)
+            # spot check: first matrix, first right-hand side
+            m0, n0, R0, C0, V0 = host[0]
+            xs = X[B.x_off[0]:B.x_off[1]].view(n0, k)[:, 0].double().cpu().numpy()
+            ys = Y[B.y_off[0]:B.y_off[1]].view(m0, k)[:, 0].double().cpu().numpy()
+            err = O.normwise_relerr(ys, O.crs_spmv_ld(O.crs(m0, n0, R0, C0, V0.astype(np.float32)), 1.0, xs, 0.0,
+                                                       np.zeros(m0)))
+            out["k"][str(k)] = {"ms": round(ms, 4), "gbs": round(byts / (ms * 1e-3) / 1e9, 1),
+                                "frac_of_hbm": round(byts / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4),
+                                "gflops": round(2 * snz * k / (ms * 1e-3) / 1e9, 1), "bytes": int(byts),
+                                "tuned_ms": round(B.tuned_ms, 4), "sell_matrices": int((B.mode == 1).sum()),
+                                "grid": B.grid, "tiles": B.ntiles, "spot_relerr": float(err)}
+            del g
+    torch.cuda.synchronize()
+    return out
+
+
+def form_adjoint(torch, pk):
+    """y = A(v) x on a random matrix (n = 1,048,576, geometric rows of mean
+    19, uniform columns, fp32 N(0,1) values): forward, dx = A^T g (values
+    refreshed through the permutation, CRS kernels on the GPU-built
+    transpose) and dvalues = g_i x_j (SDDMM); the transpose build is timed
+    once."""
+    import time as _t
+
+    from rvvlasparse_b200 import autograd as AG
+    from rvvlasparse_b200 import workloads as W
+
+    m, n, Rst, Col, Val = W.random_rows(1 << 20, 1 << 20, "geometric", 1.0 / 19.0, "normal", seed=31)
+    nnz = len(Col)
+    Rd = torch.as_tensor(Rst).cuda()
+    Cd = torch.as_tensor(Col).cuda()
+    torch.cuda.synchronize()
+    t0 = _t.perf_counter()
+    P = AG.CrsPattern(m, n, Rd, Cd, torch.float32)
+    torch.cuda.synchronize()
+    build_ms = (_t.perf_counter() - t0) * 1e3
+    v = torch.as_tensor(Val.astype(np.float32)).cuda()
+    x = torch.randn(n, device="cuda")
+    g = torch.randn(m, device="cuda")
+    fwd = 8 * nnz + 4 * (m + 1) + 4 * n + 4 * m
+    sdd = 8 * nnz + 4 * (m + 1) + 4 * m + 4 * n
+    out = {"workload": f"random rows n={m} nnz={nnz} fp32", "transpose_build_ms": round(build_ms, 2)}
+    for name, fn, b in (("forward", lambda: P.forward(v, x, 1.0), fwd), ("dx", lambda: P.adjoint_x(v, g, 1.0), fwd),
+                        ("dvalues", lambda: P.sddmm(g, x), sdd)):
+        ms = _time_ms(torch, fn)
+        out[name] = {"ms": round(ms, 4), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
+                     "frac_of_hbm": round(b / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4)}
+    return out
+
+
+def run_forms(torch, pk):
+    out = {}
+    for name, fn in (("precision", form_precision), ("batched", form_batched), ("adjoint", form_adjoint)):
+        try:
+            out[name] = fn(torch, pk)
+        except Exception as e:  # reported, never hidden
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+    return out
 
 
 def e2e_time(cases, args, torch):
@@ -399,7 +571,7 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
 
     for fmt in formats:
         for p in precs:
-            if p == "mixed" and fmt not in MIXED:
+            if p.startswith("mixed") and fmt not in MIXED:
                 continue
             # the reference has no mixed-precision kernels: its fp32 kernel
             # stands in for the mixed forms
@@ -427,7 +599,7 @@ def cpu_cases(m, n, Rst, Col, Val, formats, precs):
                 b = len(sb["vVal"]) * (vb + 4) + int(sb["cnt_b"]) * 16 + m * 4 + n * xb + m * xb
                 out.append((f"sell_{p}", O.ref_sell(sb), b, dt))
             elif fmt == "lav":
-                lb = layout("lav", dt, lambda a: O.build_lav(a, 8, 0.2, 40000))
+                lb = layout("lav", dt, lambda a: O.build_lav(a, 8, 0.2, max(n, 1)))
                 L, cc, ns, st = 8, int(lb["chunk_count"]), int(lb["segment_count"]), len(lb["mask"])
                 b = (st * L * (vb + 4) + st * 2 + ns * cc * L * 4 + (2 * cc + 1) * ns * 4 + (ns + 1) * 8
                      + crs_bytes(m, n, int(lb["sparse_nz"]), vb, xb))
@@ -523,6 +695,8 @@ def main():
     ap.add_argument("--precisions", default="f64,f32,mixed")
     ap.add_argument("--cpu-iters", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the precision (stencil), batched and adjoint forms reported under 'forms'")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -100,16 +100,19 @@ typedef struct rvvla_crs {
   const void* Val;
   const int32_t* plan;
   int64_t plan_tiles;
-  int32_t plan_kind; /* 0: merge-path tiles, 1: warp stream (no empty rows) */
+  int32_t plan_kind; /* 0: merge-path tiles, 1: warp stream, 2: warp stream over non-empty rows */
 } rvvla_crs;
 
 /* Size in int32 entries of the plan buffer for rvvla_crs_analyze (the tile
  * size depends on the value type: RVVLA_F64 or RVVLA_F32; mixed uses F32). */
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype);
-/* Analyses the row structure once (synchronises `stream`): matrices without
- * empty rows get the warp-stream split (kind 1: first row of each 2048-
- * nonzero warp range), others the merge-path split of (row ends, nonzeros)
- * (kind 0).  Writes plan[], *plan_tiles and *plan_kind for the descriptor. */
+/* Analyses the row structure once (synchronises `stream`) for the warp-
+ * stream kernel (2048 nonzeros per warp): matrices without empty rows get
+ * kind 1 (first row of each warp range; plan_tiles = warps), matrices with
+ * empty rows kind 2 (the non-empty rows compacted with a map back to their
+ * ids and the list of empty rows; plan_tiles = non-empty rows), matrices
+ * without nonzeros the merge-path split of (row ends, nonzeros) (kind 0).
+ * Writes plan[], *plan_tiles and *plan_kind for the descriptor. */
 int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* plan_tiles,
                       int32_t* plan_kind, void* stream);
 
@@ -232,6 +235,14 @@ typedef struct rvvla_lav {
   const void* val;
   const uint32_t* col_id;
   rvvla_crs sparse_part;
+  /* Optional (not in the reference class; NULL = one launch per segment):
+   * row_order[m] = the global row order the chunks are cut from, and
+   * lane_of_slot[(segment*chunk_count + chunk)*SIMD_Lanes + j] = the lane
+   * holding row_order[chunk*SIMD_Lanes + j] in that segment.  With them (and
+   * SIMD_Lanes dividing 32) one launch walks all segments and updates each
+   * row of y once. */
+  const uint32_t* row_order;
+  const uint8_t* lane_of_slot;
 } rvvla_lav;
 
 typedef struct rvvla_lav_owned {
@@ -244,6 +255,8 @@ typedef struct rvvla_lav_owned {
   uint32_t* col_id;
   int32_t *sp_Rst, *sp_Col;
   void* sp_Val;
+  uint32_t* row_order;
+  uint8_t* lane_of_slot;
 } rvvla_lav_owned;
 
 /* Builder (the reference has none; built on the host, then uploaded): dense
@@ -393,7 +406,7 @@ typedef struct rvvla_cvr_owned {
 } rvvla_cvr_owned;
 
 /* Builder (the reference has none): SIMD_LEN 32; nthreads whole-row
- * ranges balanced by nonzeros (<= 0: 2048 nonzeros each); rows enter lanes
+ * ranges balanced by nonzeros (<= 0: 32768 nonzeros each); rows enter lanes
  * longest first.  Synchronises `stream`. */
 int rvvla_cvr_build(const rvvla_crs* src, int val_bytes, int64_t nthreads, rvvla_cvr_owned* out,
                     void* stream);

@@ -623,6 +623,37 @@ int csr5_validate(const rvvla_csr5* A, const void* x, const void* y) {
   return RVVLA_OK;
 }
 
+// Warps per SM the compiled (sigma, staging) kernel keeps resident, capped at
+// 48: the SpMV launches one wave of exactly that many warps per SM (each warp
+// gets an equal share of tiles), so no partial second wave trails the grid.
+template <class V, class X, class Ac, class CT>
+int c5_resident_warps(int sigma, bool regs) {
+  static int cache[4][2] = {};
+  const int si = sigma / 8 - 1;
+  if (si < 0 || si > 3 || sigma % 8) return 48;
+  int& c = cache[si][regs ? 1 : 0];
+  if (c == 0) {
+    int blocks = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (sigma) {
+#define C5_OCC(S)                                                                                          \
+  case S:                                                                                                  \
+    e = regs ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, false>, \
+                                                            kC5Warps * 32, 0)                              \
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, true>,  \
+                                                            kC5Warps * 32, C5Cfg<V, S>::SMEM);             \
+    break;
+      C5_OCC(8)
+      C5_OCC(16)
+      C5_OCC(24)
+      C5_OCC(32)
+#undef C5_OCC
+    }
+    c = (e == cudaSuccess && blocks > 0) ? std::min(48, blocks * kC5Warps) : 48;
+  }
+  return c;
+}
+
 template <class V, class X, class Ac, class CT>
 int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaStream_t st, CT* cal_buf,
                    int* cal_row_buf, int64_t cal_cap, int* status_word, bool regs_only) {
@@ -637,7 +668,13 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
   }
   const int64_t nfull = A->p - 1;
   if (nfull > 0) {
-    const int64_t want_warps = (int64_t)sm_count() * 48;
+    // bulk copies need 16-byte aligned sources; other layouts take the
+    // register-only kernel
+    const bool aligned = ((uintptr_t)A->csr_value % 16 == 0) && ((uintptr_t)A->csr_column_index % 16 == 0) &&
+                         ((uintptr_t)A->tile_descriptor % 16 == 0);
+    const bool use_regs = regs_only || csr5_register_variant();
+    const int per_sm = aligned ? c5_resident_warps<V, X, Ac, CT>(A->sigma, use_regs) : 48;
+    const int64_t want_warps = (int64_t)sm_count() * per_sm;
     int tpw = (int)std::max<int64_t>(1, (nfull + want_warps - 1) / want_warps);
     const int64_t nwarps = (nfull + tpw - 1) / tpw;
     Scratch sc;
@@ -656,11 +693,6 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
     const V* vals = (const V*)A->csr_value;
     int* status = status_word ? status_word : device_status_word();
     if (!status) return fail(RVVLA_ERR_CUDA, "csr5: no device status word");
-    // bulk copies need 16-byte aligned sources; other layouts take the
-    // register-only kernel
-    const bool aligned = ((uintptr_t)A->csr_value % 16 == 0) && ((uintptr_t)A->csr_column_index % 16 == 0) &&
-                         ((uintptr_t)A->tile_descriptor % 16 == 0);
-    const bool use_regs = regs_only || csr5_register_variant();
     switch (aligned ? A->sigma : -1) {
 #define CSR5_CASE(S)                                                                                         \
   case S: {                                                                                                  \
@@ -795,7 +827,8 @@ int csr5_spmv_dispatch(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, c
   return csr5_spmv_impl<V, X, Ac, CT>(A, alpha, x, beta, y, st, cal, cal_row, cap, status_word, regs_only);
 }
 
-// Calibrator entries the SpMV of this matrix needs (one per warp).
+// Upper bound of the calibrator entries the SpMV of this matrix needs (one
+// per warp; the launch uses at most 48 warps per SM).
 int64_t csr5_calibrator_len(const rvvla_csr5* A) {
   const int64_t nfull = A->p - 1;
   if (nfull <= 0) return 0;

@@ -168,6 +168,15 @@ __global__ void cvr_scale_kernel(int64_t m, X* __restrict__ y, X beta) {
   if (i < m) y[i] = (beta == X(0)) ? X(0) : y[i] * beta;
 }
 
+// A warp per CVR thread (lane = SIMD lane).  Vectors are fetched kCvrU at a
+// time (independent loads in flight), records are kept in a register window
+// of 32 (lane l holds record window_base + l) and reloaded only when the
+// window is used up.  A row belongs to one lane of one range, so each row of
+// y receives exactly one contribution: y was scaled by beta first and the
+// flush is a fire-and-forget atomic add (no read of y on the critical path,
+// and still deterministic).
+constexpr int kCvrU = 4;
+
 template <class V, class X, class CT>
 __global__ void __launch_bounds__(256)
 cvr_spmv_kernel(int64_t NT, int64_t nItems, int64_t nrec, const V* __restrict__ vals,
@@ -182,42 +191,64 @@ cvr_spmv_kernel(int64_t NT, int64_t nItems, int64_t nrec, const V* __restrict__ 
   const int64_t re = (t + 1 < NT) ? wb[(t + 1) * (kS + 2) + 1] : nrec;
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
   CT res = 0;
-  int64_t rc = rb;
   s_row[w][lane] = -1;
   __syncwarp();
+  int64_t wbase = rb;
+  int cons = 0;
+  int navail = (int)(re - wbase < 0 ? 0 : (re - wbase > kS ? kS : re - wbase));
+  int my_pos = lane < navail ? rec[2 * (wbase + lane)] : INT_MAX;
+  int my_row = lane < navail ? rec[2 * (wbase + lane) + 1] : -1;
   // apply the records whose position falls before `limit`
   auto apply = [&](int64_t limit) {
     for (;;) {
-      const int64_t j = rc + lane;
-      const bool have = j < re;
-      const int pos = have ? rec[2 * j] : INT_MAX;
-      const bool take = have && (int64_t)pos < limit;
+      if (cons == navail) {
+        if (navail < kS) return;  // no records left in this range
+        wbase += kS;
+        cons = 0;
+        navail = (int)(re - wbase < 0 ? 0 : (re - wbase > kS ? kS : re - wbase));
+        if (navail == 0) return;
+        my_pos = lane < navail ? rec[2 * (wbase + lane)] : INT_MAX;
+        my_row = lane < navail ? rec[2 * (wbase + lane) + 1] : -1;
+      }
+      const bool take = lane >= cons && lane < navail && (int64_t)my_pos < limit;
       const unsigned mk = __ballot_sync(0xffffffffu, take);
-      if (!mk) break;
-      if (take) s_row[w][pos % kS] = rec[2 * j + 1];
+      if (!mk) return;
+      if (take) s_row[w][my_pos % kS] = my_row;
       __syncwarp();
       const int r = s_row[w][lane];
       if (r >= 0) {
-        if (res != CT(0)) y[r] += alpha * (X)res;
+        if (res != CT(0)) atomicAdd(y + r, alpha * (X)res);
         res = 0;
         s_row[w][lane] = -1;
       }
       __syncwarp();
-      const int cnt = __popc(mk);
-      rc += cnt;
-      if (cnt < 32) break;
+      cons += __popc(mk);
+      if (cons < navail) return;  // stopped at a record past the limit
     }
   };
-  for (int64_t v = vb; v < ve; ++v) {
-    apply(v * kS + kS);
-    const int64_t k = v * kS + lane;
-    const uint32_t c = ld_stream(cols + k, pf);
-    res += (CT)vmul(ld_stream(vals + k, pf), ld_keep(x + c, pl));
+  for (int64_t v = vb; v < ve; v += kCvrU) {
+    CT p[kCvrU];
+#pragma unroll
+    for (int u = 0; u < kCvrU; ++u) {
+      p[u] = 0;
+      if (v + u < ve) {
+        const int64_t k = (v + u) * kS + lane;
+        const uint32_t c = ld_stream(cols + k, pf);
+        p[u] = (CT)vmul(ld_stream(vals + k, pf), ld_keep(x + c, pl));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kCvrU; ++u) {
+      if (v + u < ve) {
+        apply((v + u) * kS + kS);
+        res += p[u];
+      }
+    }
   }
   apply(INT64_MAX);
   if (t + 1 == NT) {  // the last range's tail rows
     const int r = wb[t * (kS + 2) + 2 + lane];
-    if (res != CT(0)) y[r] += alpha * (X)res;
+    if (res != CT(0)) atomicAdd(y + r, alpha * (X)res);
   }
 }
 
@@ -252,7 +283,10 @@ int cvr_build_impl(const rvvla_crs* src, int vb, int64_t NT, rvvla_cvr_owned* ou
   if (vb != 8 && vb != 4 && vb != 2) return fail(RVVLA_ERR_INVALID_ARG, "cvr_build: val_bytes must be 8, 4 or 2");
   const int64_t m = src->m, nnz = src->nz;
   if (m < 0 || nnz < 0 || src->n < 0) return fail(RVVLA_ERR_INVALID_ARG, "cvr_build: bad sizes");
-  if (NT <= 0) NT = std::max<int64_t>(1, (nnz + 2047) / 2048);
+  // ranges of ~32K nonzeros: smaller ranges drain their lanes unevenly and
+  // pad the vectors (2K nonzeros per range triples the stored items on a
+  // power-law matrix, 32K adds ~3 %)
+  if (NT <= 0) NT = std::max<int64_t>(1, (nnz + 32767) / 32768);
   if (nnz >= INT32_MAX / 2 || m >= INT32_MAX) return fail(RVVLA_ERR_TOO_LARGE, "cvr_build: sizes beyond int32 records");
   rvvla_cvr& h = out->h;
   h.numRows = m; h.numCols = src->n; h.SIMD_LEN = kS; h.Nthreads = (int32_t)NT; h.Nthreads_avail = (int32_t)NT;

@@ -24,7 +24,10 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
+#include "crs_merge.cuh"
+#include "crs_stream.cuh"
 #include "rvvla_internal.cuh"
 #include "scan.cuh"
 
@@ -191,6 +194,31 @@ __device__ __forceinline__ int find_slot(const int* pre, int n, int v) {
   return lo;
 }
 
+// Number of lanes l whose (non-decreasing across lanes) value b_l is <= q,
+// for each lane's own q: a binary search over the warp by shuffles.
+__device__ __forceinline__ int warp_count_le(int b, int q) {
+  const int b31 = __shfl_sync(0xffffffffu, b, 31);
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int v = __shfl_sync(0xffffffffu, b, lo + step - 1);
+    if (v <= q) lo += step;
+  }
+  if (lo == 31 && b31 <= q) lo = 32;
+  return lo;
+}
+
+template <class V>
+__device__ __forceinline__ V ldval(const V* p, uint64_t pol) { return ld_stream(p, pol); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 ldval<__nv_bfloat16>(const __nv_bfloat16* p, uint64_t) { return ldv(p); }
+
+template <bool MIX, class V, class X>
+__device__ __forceinline__ auto hprod(V v, X x) {
+  if constexpr (MIX) return to_float(v) * (float)x;
+  else return v * x;
+}
+
 // V stored value, X vector type, SA shared accumulator type, MIX: compensated
 // fp32 row sums merged into fp64.
 //
@@ -208,6 +236,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
                  const uint32_t* __restrict__ row_offset, const uint32_t* __restrict__ row_ptr,
                  const uint16_t* __restrict__ col_idx, const V* __restrict__ values, const X* __restrict__ x,
                  X* __restrict__ y, X alpha, X beta) {
+  using Ac = std::conditional_t<MIX, CompF32, SA>;
   extern __shared__ __align__(16) unsigned char smem[];
   SA* acc = reinterpret_cast<SA*>(smem);
   int* csr_pre = reinterpret_cast<int*>(smem + ((R * sizeof(SA) + 15) / 16) * 16);
@@ -252,40 +281,61 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
   }
   const int n_csr = carry_a, n_coo = carry_b;
   const int total = n_csr + ((n_coo + 31) >> 5);
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
   for (int item = warp; item < total; item += kHcsrWarps) {
     if (item < n_csr) {
+      // 32 rows of a CSR block: their nonzeros are contiguous, so the warp
+      // streams them in coalesced chunks of 32; lane l holds the start of row
+      // l, a shuffle search gives each nonzero its row, and a segmented
+      // warp sum leaves one shared-memory add per row piece
       const int64_t j = find_slot(csr_pre, (int)b_n, item);
       const int part = item - csr_pre[j];
       const int64_t blk = blk0 + j;
       const uint32_t off = row_offset[blk] & kKindMask;
       const int bp = block_ptr[blk];
       const X* xb = x + j * C;
-      const int li = part * 32 + lane;
-      if (li < maxr) {
-        const uint32_t qb = row_ptr[off + li], qe = row_ptr[off + li + 1];
-        if constexpr (MIX) {
-          CompF32 s;
-          for (uint32_t q = qb; q < qe; ++q) s.add(to_float(ldv(values + bp + q)) * (float)ldx(xb + col_idx[bp + q]));
-          atomicAdd(&acc[li], (SA)((double)s.s + (double)s.c));
-        } else {
-          SA s = 0;
-          for (uint32_t q = qb; q < qe; ++q) s += (SA)ldv(values + bp + q) * (SA)ldx(xb + col_idx[bp + q]);
-          atomicAdd(&acc[li], s);
-        }
+      const int li0 = part * 32;
+      const int nr = min(32, maxr - li0);
+      const int rs = (lane < nr) ? (int)row_ptr[off + li0 + lane] : INT_MAX;
+      const int e_beg = __shfl_sync(0xffffffffu, rs, 0);
+      const int e_end = (int)row_ptr[off + li0 + nr];
+      for (int cb = e_beg; cb < e_end; cb += 32) {
+        const int e = cb + lane;
+        const bool valid = e < e_end;
+        const int r = warp_count_le(rs, e) - 1;  // row of nonzero e within the item
+        Ac pr;
+        acc_zero(pr);
+        if (valid) acc_add(pr, hprod<MIX>(ldval(values + bp + e, pf), ld_keep(xb + col_idx[bp + e], pl)));
+        const int rp = __shfl_up_sync(0xffffffffu, r, 1);
+        const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || r != rp);
+        const Ac sc = acc_seg_scan(pr, heads, lane);
+        const int last_valid = min(31, e_end - 1 - cb);
+        const bool next_head = lane < 31 && ((heads >> (lane + 1)) & 1u);
+        if (valid && ((int)lane == last_valid || next_head)) atomicAdd(&acc[li0 + r], (SA)acc_carry(sc));
       }
     } else {
-      const int q = ((item - n_csr) << 5) + lane;
+      // 32 COO nonzeros of the block-row (blocks taken in order): lane 0
+      // finds the block of the first one, lanes hold the next 32 block
+      // boundaries and a shuffle search places every nonzero
+      const int q0 = (item - n_csr) << 5;
+      const int q = q0 + lane;
+      int j0 = 0;
+      if (lane == 0) j0 = find_slot(coo_pre, (int)b_n, q0);
+      j0 = __shfl_sync(0xffffffffu, j0, 0);
+      const int bnd = (j0 + 1 + lane <= b_n) ? coo_pre[j0 + 1 + lane] : INT_MAX;
+      int k = warp_count_le(bnd, q);
+      int64_t j = j0 + k;
+      if (k == 32) j = find_slot(coo_pre, (int)b_n, q);  // more than 32 blocks in reach
       if (q < n_coo) {
-        const int64_t j = find_slot(coo_pre, (int)b_n, q);
         const int64_t blk = blk0 + j;
-        const int k = q - coo_pre[j];
+        const int kk = q - coo_pre[j];
         const uint32_t off = row_offset[blk] & kKindMask;
-        const int e = block_ptr[blk] + k;
-        const uint32_t li = row_ptr[off + k];
-        const X xv = ldx(x + j * C + col_idx[e]);
+        const int e = block_ptr[blk] + kk;
+        const uint32_t li = row_ptr[off + kk];
+        const X xv = ld_keep(x + j * C + col_idx[e], pl);
         SA p;
         if constexpr (MIX) p = (SA)(to_float(ldv(values + e)) * (float)xv);
-        else p = (SA)ldv(values + e) * (SA)xv;
+        else p = (SA)ldval(values + e, pf) * (SA)xv;
         atomicAdd(&acc[li], p);
       }
     }

@@ -63,6 +63,71 @@ lav_segment_kernel(int64_t s, int64_t L, int64_t cc, const int* __restrict__ co,
   y[r] += alpha * (X)acc;
 }
 
+// All segments in one pass (L divides 32): lane (c, j) of a warp owns slot j
+// of chunk c, i.e. row row_order[c*L + j].  In every segment lane (c, i)
+// sums its steps for the row the segment placed at lane i, and the slot
+// owner takes that sum from lane lane_of_slot[(s, c, j)] with a shuffle, so a
+// row's segment sums are added in registers in segment order and y is
+// read-modified-written once (after the sparse part has applied beta).
+template <class V, class X, class CT, int L>
+__global__ void __launch_bounds__(256)
+lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, const int* __restrict__ co, const int* __restrict__ cf,
+                 const uint64_t* __restrict__ sp, const uint16_t* __restrict__ mk, const V* __restrict__ val,
+                 const uint32_t* __restrict__ col, const uint8_t* __restrict__ los,
+                 const uint32_t* __restrict__ row_order, const X* __restrict__ x, X* __restrict__ y, X alpha) {
+  static_assert(32 % L == 0, "a chunk must not straddle warps");
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t c = gid / L;
+  const int i = (int)(gid % L);
+  const bool live = c < cc;
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+  CT acc = 0;
+  for (int64_t s = 0; s < nseg; ++s) {
+    CT part = 0;
+    int src = i;
+    if (live) {
+      const int64_t sh = (cc + 1) * s;
+      const int st = co[sh + c], en = co[sh + c + 1];
+      if (st < en) {
+        const int fe = cf[s * cc + c];
+        const int64_t base = (int64_t)sp[s];
+        src = los[(s * cc + c) * L + i];
+        // steps four at a time (independent loads in flight); a step is
+        // active for every lane before fe, and for the first mask[q] lanes
+        // after it
+        for (int q0 = st; q0 < en; q0 += 4) {
+          bool act[4];
+          uint32_t ci[4];
+          V vv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int q = q0 + u;
+            act[u] = q < en && (q < fe || i < (int)mk[base + q]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (act[u]) {
+              const int64_t e = (base + q0 + u) * L + i;
+              ci[u] = ld_stream(col + e, pf);
+              vv[u] = ld_stream(val + e, pf);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (act[u]) part += (CT)vmul(vv[u], ld_keep(x + ci[u], pl));
+        }
+      }
+    }
+    acc += __shfl_sync(0xffffffffu, part, (lane & ~(L - 1)) + src);
+  }
+  const int64_t g = c * L + i;
+  if (live && g < m) {
+    const uint32_t r = row_order[g];
+    y[r] += alpha * (X)acc;
+  }
+}
+
 template <class T>
 int upload(const std::vector<T>& v, T** dst, cudaStream_t st) {
   RVVLA_CUDA(cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)));
@@ -91,11 +156,15 @@ int lav_build_typed(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen
       (rc = upload(H.sp, &out->segment_ptr, st)) || (rc = upload(H.oo, &out->out_order, st)) ||
       (rc = upload(H.mk, &out->mask, st)) || (rc = upload(H.val, reinterpret_cast<T**>(&out->val), st)) ||
       (rc = upload(H.col, &out->col_id, st)) || (rc = upload(H.sRst, &out->sp_Rst, st)) ||
-      (rc = upload(H.sCol, &out->sp_Col, st)) || (rc = upload(H.sVal, reinterpret_cast<T**>(&out->sp_Val), st)))
+      (rc = upload(H.sCol, &out->sp_Col, st)) || (rc = upload(H.sVal, reinterpret_cast<T**>(&out->sp_Val), st)) ||
+      (rc = upload(H.row_order, &out->row_order, st)))
     return rc;
+  if (!H.lane_of_slot.empty() && (rc = upload(H.lane_of_slot, &out->lane_of_slot, st))) return rc;
   h.chunk_offsets = out->chunk_offsets; h.chunk_offsets_full_mask = out->chunk_offsets_full_mask;
   h.segment_ptr = out->segment_ptr; h.out_order = out->out_order; h.mask = out->mask; h.val = out->val;
   h.col_id = out->col_id;
+  h.row_order = out->row_order;
+  h.lane_of_slot = out->lane_of_slot;
   h.sparse_part.m = m; h.sparse_part.n = src->n; h.sparse_part.nz = (int64_t)H.sCol.size();
   h.sparse_part.Rst = out->sp_Rst; h.sparse_part.Col = out->sp_Col; h.sparse_part.Val = out->sp_Val;
   h.sparse_part.plan = nullptr; h.sparse_part.plan_tiles = 0; h.sparse_part.plan_kind = 0;
@@ -114,6 +183,30 @@ int lav_spmv_impl(const rvvla_lav* A, X alpha, const X* x, X beta, X* y, cudaStr
   int rc = crs_fn(&A->sparse_part, alpha, x, beta, y, (void*)st);
   if (rc) return rc;
   const int64_t threads = A->chunk_count * A->SIMD_Lanes;
+  if (A->segment_count == 0) return RVVLA_OK;
+  if (A->row_order && A->lane_of_slot && A->SIMD_Lanes <= 32 && 32 % A->SIMD_Lanes == 0) {
+    const int64_t total = (threads + 31) / 32 * 32;  // whole warps: every lane takes part in the shuffles
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    switch (A->SIMD_Lanes) {
+#define LAV_FUSED(LN)                                                                                          \
+  case LN:                                                                                                     \
+    lav_fused_kernel<V, X, CT, LN><<<blocks, 256, 0, st>>>(A->segment_count, A->chunk_count, A->m,             \
+                                                          A->chunk_offsets, A->chunk_offsets_full_mask,       \
+                                                          A->segment_ptr, A->mask, (const V*)A->val,          \
+                                                          A->col_id, A->lane_of_slot, A->row_order, x, y,     \
+                                                          alpha);                                             \
+    break;
+      LAV_FUSED(1)
+      LAV_FUSED(2)
+      LAV_FUSED(4)
+      LAV_FUSED(8)
+      LAV_FUSED(16)
+      LAV_FUSED(32)
+#undef LAV_FUSED
+    }
+    RVVLA_LAUNCHED("lav_fused_kernel");
+    return RVVLA_OK;
+  }
   for (int64_t s = 0; s < A->segment_count; ++s) {
     lav_segment_kernel<V, X, CT><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
         s, A->SIMD_Lanes, A->chunk_count, A->chunk_offsets, A->chunk_offsets_full_mask, A->segment_ptr, A->out_order,
@@ -152,7 +245,7 @@ int rvvla_lav_build(const rvvla_crs* src, int val_bytes, int64_t simd_lanes, dou
 void rvvla_lav_free(rvvla_lav_owned* h) {
   if (!h) return;
   void* ptrs[] = {h->chunk_offsets, h->chunk_offsets_full_mask, h->segment_ptr, h->out_order, h->mask, h->val,
-                  h->col_id, h->sp_Rst, h->sp_Col, h->sp_Val};
+                  h->col_id, h->sp_Rst, h->sp_Col, h->sp_Val, h->row_order, h->lane_of_slot};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   std::memset(h, 0, sizeof(*h));

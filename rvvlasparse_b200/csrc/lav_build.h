@@ -32,6 +32,11 @@ struct LavHost {
   std::vector<uint32_t> oo, col;
   std::vector<uint16_t> mk;
   std::vector<T> val, sVal;
+  // derived for the one-pass GPU kernel (not part of the reference layout):
+  // the global row order, and per (segment, chunk, slot j) the lane that
+  // holds row_order[chunk*L + j] in that segment (only for L <= 256)
+  std::vector<uint32_t> row_order;
+  std::vector<uint8_t> lane_of_slot;
 };
 
 template <class T>
@@ -88,6 +93,7 @@ void lav_build_host(const int* Rst, const int* Col, const T* Val, int64_t m, int
   std::vector<uint32_t> gorder((size_t)m);
   std::iota(gorder.begin(), gorder.end(), 0u);
   std::stable_sort(gorder.begin(), gorder.end(), [&](uint32_t a, uint32_t b) { return dcount[a] > dcount[b]; });
+  o.row_order = gorder;
   o.co.assign((size_t)((cc + 1) * nseg), 0);
   o.cf.assign((size_t)(cc * nseg), 0);
   o.sp.assign((size_t)nseg + 1, 0);
@@ -156,6 +162,20 @@ void lav_build_host(const int* Rst, const int* Col, const T* Val, int64_t m, int
           }
         }
       }
+    }
+  }
+  // slot -> lane map (identity for the padding slots of the last chunk)
+  if (L <= 256) {
+    std::vector<uint8_t> slot_of((size_t)m);
+    for (int64_t g = 0; g < m; ++g) slot_of[o.row_order[(size_t)g]] = (uint8_t)(g % L);
+    o.lane_of_slot.assign((size_t)(nseg * cc * L), 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < nseg * cc; ++q) {
+      const int64_t c = q % cc;
+      const int64_t nrows = std::min(m, (c + 1) * L) - c * L;
+      uint8_t* lo = &o.lane_of_slot[(size_t)(q * L)];
+      for (int64_t i = 0; i < L; ++i) lo[i] = (uint8_t)i;
+      for (int64_t i = 0; i < nrows; ++i) lo[slot_of[o.oo[(size_t)(q * L + i)]]] = (uint8_t)i;
     }
   }
 }

@@ -123,6 +123,91 @@ sell_spmv_kernel(int64_t m, int64_t C, const int* __restrict__ vCl, const int* _
   write_row(y, (int)out, alpha, beta, (X)acc_out(acc));
 }
 
+// C == 32: a warp per slice (lane = row of the slice, column-major loads are
+// coalesced).  A CTA covers 8 consecutive slices; slices wider than
+// kSellWide columns (the long rows that sigma-sorting gathers at the head of
+// a window) are shared by all 8 warps of the CTA, each taking every eighth
+// group of 4 columns, and the 8 partial sums of a row are merged in warp
+// order through shared memory, so a wide slice costs the CTA width/8 steps
+// instead of holding one warp for width steps.
+constexpr int kSellWide = 64;
+
+template <class V, class X, class Ac, int MODE>
+__global__ void __launch_bounds__(256)
+sell_warp_kernel(int64_t cnt_b, const int* __restrict__ vCl, const int* __restrict__ vCs,
+                 const int* __restrict__ vBs, const int* __restrict__ vSBs, const uint32_t* __restrict__ vCol,
+                 const uint32_t* __restrict__ vPerm, const V* __restrict__ vVal, const X* __restrict__ x,
+                 X* __restrict__ y, X alpha, X beta) {
+  __shared__ Ac red[8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t s0 = (int64_t)blockIdx.x * 8;
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+  {
+    const int64_t s = s0 + warp;
+    if (s < cnt_b) {
+      const int w = vCl[s], bs = vBs[s];
+      if (w <= kSellWide && lane < bs) {
+        const int64_t base = vCs[s] + lane;
+        Ac acc;
+        acc_zero(acc);
+        int j = 0;
+        for (; j + 4 <= w; j += 4) {
+          uint32_t c[4];
+          V v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            c[u] = ld_stream(vCol + base + (int64_t)(j + u) * bs, pf);
+            v[u] = ld_stream(vVal + base + (int64_t)(j + u) * bs, pf);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) acc_add(acc, vmul(v[u], ld_keep(x + c[u], pl)));
+        }
+        for (; j < w; ++j) {
+          const uint32_t c = ld_stream(vCol + base + (int64_t)j * bs, pf);
+          acc_add(acc, vmul(ld_stream(vVal + base + (int64_t)j * bs, pf), ld_keep(x + c, pl)));
+        }
+        const int64_t out = (MODE == 1) ? (int64_t)vPerm[vSBs[s] + lane] : (int64_t)vSBs[s] + lane;
+        write_row(y, (int)out, alpha, beta, (X)acc_out(acc));
+      }
+    }
+  }
+  for (int q = 0; q < 8; ++q) {  // wide slices: the whole CTA (uniform branches)
+    const int64_t s = s0 + q;
+    if (s >= cnt_b) break;
+    const int w = vCl[s];
+    if (w <= kSellWide) continue;
+    const int bs = vBs[s];
+    Ac acc;
+    acc_zero(acc);
+    if (lane < bs) {
+      const int64_t base = vCs[s] + lane;
+      for (int j0 = warp * 4; j0 < w; j0 += 32) {
+        uint32_t c[4];
+        V v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const bool in = j0 + u < w;
+          c[u] = in ? ld_stream(vCol + base + (int64_t)(j0 + u) * bs, pf) : 0u;
+          v[u] = in ? ld_stream(vVal + base + (int64_t)(j0 + u) * bs, pf) : V(0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (j0 + u < w) acc_add(acc, vmul(v[u], ld_keep(x + c[u], pl)));
+      }
+    }
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0 && lane < bs) {
+      Ac t = red[0][lane];
+#pragma unroll
+      for (int k = 1; k < 8; ++k) acc_merge(t, red[k][lane]);
+      const int64_t out = (MODE == 1) ? (int64_t)vPerm[vSBs[s] + lane] : (int64_t)vSBs[s] + lane;
+      write_row(y, (int)out, alpha, beta, (X)acc_out(t));
+    }
+    __syncthreads();
+  }
+}
+
 template <class X>
 __global__ void sell_permute_kernel(int64_t m, const uint32_t* __restrict__ perm, const X* __restrict__ src,
                                     X* __restrict__ dst, int gather) {
@@ -159,6 +244,17 @@ int sell_spmv_impl(const rvvla_sell* A, int stage, X alpha, const X* x, X beta, 
     return RVVLA_OK;
   }
   const V* vv = (const V*)A->vVal;
+  if (A->C == 32 && (stage == RVVLA_STAGE_MULT || stage == RVVLA_STAGE_ALL)) {
+    const unsigned wblocks = (unsigned)((A->cnt_b + 7) / 8);
+    if (stage == RVVLA_STAGE_MULT)
+      sell_warp_kernel<V, X, Ac, 0><<<wblocks, 256, 0, st>>>(A->cnt_b, A->vCl, A->vCs, A->vBs, A->vSBs, A->vCol,
+                                                             A->vPerm, vv, x, y, alpha, beta);
+    else
+      sell_warp_kernel<V, X, Ac, 1><<<wblocks, 256, 0, st>>>(A->cnt_b, A->vCl, A->vCs, A->vBs, A->vSBs, A->vCol,
+                                                             A->vPerm, vv, x, y, alpha, beta);
+    RVVLA_LAUNCHED("sell_warp_kernel");
+    return RVVLA_OK;
+  }
   if (stage == RVVLA_STAGE_MULT)
     sell_spmv_kernel<V, X, Ac, 0><<<blocks, 256, 0, st>>>(A->m, A->C, A->vCl, A->vCs, A->vBs, A->vSBs, A->vCol,
                                                           A->vPerm, vv, x, y, alpha, beta);

@@ -357,7 +357,8 @@ class spMtxLAV(_GpuFormat):
 
     SCALARS = ("SIMD_Lanes", "m", "n", "nz", "segment_count", "chunk_count", "segment_len", "n_steps")
     ARRAYS = {"chunk_offsets": torch.int32, "chunk_offsets_full_mask": torch.int32, "segment_ptr": torch.int64,
-              "out_order": torch.int32, "mask": torch.int16, "val": None, "col_id": torch.int32}
+              "out_order": torch.int32, "mask": torch.int16, "val": None, "col_id": torch.int32,
+              "row_order": torch.int32, "lane_of_slot": torch.uint8}
     CDESC = _capi.rvvla_lav
     VALUE = "val"
 
@@ -401,7 +402,10 @@ def _lav_convert(dist, src: spMtxCRS, params: convertParams) -> None:
         h = owned.h
         L, cc, ns = h.SIMD_Lanes, h.chunk_count, h.segment_count
         sizes = {"chunk_offsets": (cc + 1) * ns, "chunk_offsets_full_mask": cc * ns, "segment_ptr": ns + 1,
-                 "out_order": ns * cc * L, "mask": h.n_steps, "val": h.n_steps * L, "col_id": h.n_steps * L}
+                 "out_order": ns * cc * L, "mask": h.n_steps, "val": h.n_steps * L, "col_id": h.n_steps * L,
+                 "row_order": h.m}
+        if owned.lane_of_slot:  # derived slot -> lane map (SIMD_Lanes <= 256)
+            sizes["lane_of_slot"] = ns * cc * L
         dist._adopt(owned, sizes, src.Val.dtype, src.Val.device)
         dist.T = float(h.T)
         dev = src.Val.device

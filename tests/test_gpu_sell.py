@@ -106,3 +106,19 @@ def test_sell_mixed_within_1e6():
     S = build(m, n, Rst, Col, Val.astype(np.float32))
     y = run(S, 1.0, x.astype(np.float32), 0.0, np.zeros(m, np.float32), mixed=True)
     assert O.normwise_relerr(y, yref) <= 1e-6
+
+
+@pytest.mark.parametrize("C,sigma", [(32, 64), (32, 1)])
+def test_sell_warp_slices_all_and_staged(g, C, sigma):
+    """C = 32 runs the warp-per-slice kernel; slices wider than 64 columns
+    (one_long_row, powerlaw1k) are shared by the whole CTA."""
+    S = build(g["m"], g["n"], g["Rst"], g["Col"], g["Val"], C, sigma)
+    tol = tol_for(g["Val"].dtype)
+    yref = O.crs_spmv_ld(O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"]), g["alpha"], g["x"], g["beta"], g["y0"])
+    y_all = run(S, g["alpha"], g["x"], g["beta"], g["y0"])
+    assert O.normwise_relerr(y_all, yref) < tol
+    y = dev(g["y0"])
+    for st in (R.SPARSE_MATRIX_MV_PREPARATION, R.SPARSE_MATRIX_MV_MULT, R.SPARSE_MATRIX_MV_GET_RESULTS):
+        assert R.sparse_mv(NT, g["alpha"], S, R.sparse_matrix_descr(), dev(g["x"]), g["beta"], y, st).code == 0
+    torch.cuda.synchronize()
+    assert O.normwise_relerr(y.cpu().numpy(), yref) < tol
