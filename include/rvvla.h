@@ -240,9 +240,12 @@ typedef struct rvvla_lav {
    * lane_of_slot[(segment*chunk_count + chunk)*SIMD_Lanes + j] = the lane
    * holding row_order[chunk*SIMD_Lanes + j] in that segment.  With them (and
    * SIMD_Lanes dividing 32) one launch walks all segments and updates each
-   * row of y once. */
+   * row of y once.  long_chunks (0 = none): the leading chunks that get a
+   * thread block each, their steps spread over the block (the builder sets
+   * it to cover the chunks of >= 128 steps). */
   const uint32_t* row_order;
   const uint8_t* lane_of_slot;
+  int64_t long_chunks;
 } rvvla_lav;
 
 typedef struct rvvla_lav_owned {
@@ -406,7 +409,7 @@ typedef struct rvvla_cvr_owned {
 } rvvla_cvr_owned;
 
 /* Builder (the reference has none): SIMD_LEN 32; nthreads whole-row
- * ranges balanced by nonzeros (<= 0: 32768 nonzeros each); rows enter lanes
+ * ranges balanced by nonzeros (<= 0: 16384 nonzeros each); rows enter lanes
  * longest first.  Synchronises `stream`. */
 int rvvla_cvr_build(const rvvla_crs* src, int val_bytes, int64_t nthreads, rvvla_cvr_owned* out,
                     void* stream);

@@ -82,7 +82,8 @@ class rvvla_lav(C.Structure):
     _fields_ = [("SIMD_Lanes", i64), ("m", i64), ("n", i64), ("nz", i64), ("segment_count", i64),
                 ("chunk_count", i64), ("segment_len", i64), ("n_steps", i64), ("T", dbl), ("chunk_offsets", vp),
                 ("chunk_offsets_full_mask", vp), ("segment_ptr", vp), ("out_order", vp), ("mask", vp), ("val", vp),
-                ("col_id", vp), ("sparse_part", rvvla_crs), ("row_order", vp), ("lane_of_slot", vp)]
+                ("col_id", vp), ("sparse_part", rvvla_crs), ("row_order", vp), ("lane_of_slot", vp),
+                ("long_chunks", i64)]
 
 
 class rvvla_lav_owned(C.Structure):

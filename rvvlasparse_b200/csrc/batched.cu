@@ -61,9 +61,13 @@ __device__ __forceinline__ void store_y(T* y, T alpha, T beta, T v) {
   *y = (beta == T(0)) ? alpha * v : alpha * v + beta * *y;
 }
 
+// The row pointers of the tile are staged in shared memory first (one
+// coalesced load), so no row waits on a dependent row-pointer load.
+constexpr int kTileRowsMax = 2048;
+
 template <class T>
-__device__ void csr_k1(const BatchMat& A, const BatchTile& t, const T* __restrict__ X, T* __restrict__ Y, T alpha,
-                       T beta) {
+__device__ void csr_k1(const BatchMat& A, const BatchTile& t, const int* __restrict__ srst, const T* __restrict__ X,
+                       T* __restrict__ Y, T alpha, T beta) {
   const int tpr = A.tpr;
   const int slot = threadIdx.x / tpr, lane = threadIdx.x % tpr, nslots = kBThreads / tpr;
   const T* __restrict__ x = X + A.x_off;
@@ -75,63 +79,92 @@ __device__ void csr_k1(const BatchMat& A, const BatchTile& t, const T* __restric
   for (int it = 0; it < iters; ++it) {
     const int rr = it * nslots + slot;
     const bool valid = rr < t.count;
-    const int r = t.first + rr;
-    T s = T(0);
+    T s0 = T(0), s1 = T(0);
     if (valid) {
-      const int b = A.Rst[r], e = A.Rst[r + 1];
-      for (int j = b + lane; j < e; j += tpr) s += ld_stream(val + j, pf) * ld_keep(x + ld_stream(A.Col + j, pf), pl);
+      const int b = srst[rr], e = srst[rr + 1];
+      int j = b + lane;
+      for (; j + tpr < e; j += 2 * tpr) {
+        const int c0 = ld_stream(A.Col + j, pf), c1 = ld_stream(A.Col + j + tpr, pf);
+        const T v0 = ld_stream(val + j, pf), v1 = ld_stream(val + j + tpr, pf);
+        s0 += v0 * ld_keep(x + c0, pl);
+        s1 += v1 * ld_keep(x + c1, pl);
+      }
+      if (j < e) s0 += ld_stream(val + j, pf) * ld_keep(x + ld_stream(A.Col + j, pf), pl);
     }
+    T s = s0 + s1;
     for (int off = tpr >> 1; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off, tpr);
-    if (valid && lane == 0) store_y(Y + A.y_off + r, alpha, beta, s);
+    if (valid && lane == 0) store_y(Y + A.y_off + t.first + rr, alpha, beta, s);
   }
 }
 
 template <class T, int K>
-__device__ void csr_kn(const BatchMat& A, const BatchTile& t, const T* __restrict__ X, T* __restrict__ Y, T alpha,
-                       T beta) {
+__device__ void csr_kn(const BatchMat& A, const BatchTile& t, const int* __restrict__ srst, const T* __restrict__ X,
+                       T* __restrict__ Y, T alpha, T beta) {
   constexpr int nslots = kBThreads / K;
   const int slot = threadIdx.x / K, rhs = threadIdx.x % K;
   const T* __restrict__ x = X + A.x_off + rhs;
   const T* __restrict__ val = static_cast<const T*>(A.Val);
   const uint64_t pl = policy_evict_last();
   for (int rr = slot; rr < t.count; rr += nslots) {
-    const int r = t.first + rr;
-    const int b = A.Rst[r], e = A.Rst[r + 1];
-    T s0 = T(0), s1 = T(0);
+    const int b = srst[rr], e = srst[rr + 1];
+    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
     int j = b;
-    for (; j + 1 < e; j += 2) {
-      const int c0 = A.Col[j], c1 = A.Col[j + 1];
-      const T v0 = val[j], v1 = val[j + 1];
+    for (; j + 3 < e; j += 4) {
+      const int c0 = A.Col[j], c1 = A.Col[j + 1], c2 = A.Col[j + 2], c3 = A.Col[j + 3];
+      const T v0 = val[j], v1 = val[j + 1], v2 = val[j + 2], v3 = val[j + 3];
       s0 += v0 * ld_keep(x + (int64_t)c0 * K, pl);
       s1 += v1 * ld_keep(x + (int64_t)c1 * K, pl);
+      s2 += v2 * ld_keep(x + (int64_t)c2 * K, pl);
+      s3 += v3 * ld_keep(x + (int64_t)c3 * K, pl);
     }
-    if (j < e) s0 += val[j] * ld_keep(x + (int64_t)A.Col[j] * K, pl);
-    store_y(Y + A.y_off + (int64_t)r * K + rhs, alpha, beta, s0 + s1);
+    for (; j < e; ++j) s0 += val[j] * ld_keep(x + (int64_t)A.Col[j] * K, pl);
+    store_y(Y + A.y_off + (int64_t)(t.first + rr) * K + rhs, alpha, beta, (s0 + s1) + (s2 + s3));
   }
 }
 
+// Slice metadata of a SELL tile (height, width, start, first sorted row),
+// staged in shared memory so a slice starts without dependent loads.
+constexpr int kTileSlicesMax = kBWarps * 4;
+
 template <class T, int K>
-__device__ void sell_kn(const BatchMat& A, const BatchTile& t, const T* __restrict__ X, T* __restrict__ Y, T alpha,
-                        T beta) {
+__device__ void sell_kn(const BatchMat& A, const BatchTile& t, const int (*meta)[kTileSlicesMax],
+                        const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta) {
+  constexpr int U = (K == 1) ? 8 : 4;  // columns in flight
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const T* __restrict__ val = static_cast<const T*>(A.sVal);
   const T* __restrict__ x = X + A.x_off;
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
   for (int q = warp; q < t.count; q += kBWarps) {
-    const int sl = t.first + q;
-    const int h = A.sBs[sl], w = A.sCl[sl], base = A.sCs[sl];
+    const int h = meta[0][q], w = meta[1][q], base = meta[2][q];
     if (lane >= h) continue;
+    const int row = (int)A.sPerm[meta[3][q] + lane];
     T acc[K];
 #pragma unroll
     for (int i = 0; i < K; ++i) acc[i] = T(0);
-    for (int j = 0; j < w; ++j) {
+    int j = 0;
+    for (; j + U <= w; j += U) {
+      T v[U];
+      uint32_t c[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t idx = (int64_t)base + (int64_t)(j + u) * h + lane;
+        v[u] = ld_stream(val + idx, pf);
+        c[u] = ld_stream(A.sCol + idx, pf);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const T* xr = x + (int64_t)c[u] * K;
+#pragma unroll
+        for (int i = 0; i < K; ++i) acc[i] += v[u] * ld_keep(xr + i, pl);
+      }
+    }
+    for (; j < w; ++j) {
       const int64_t idx = (int64_t)base + (int64_t)j * h + lane;
       const T v = ld_stream(val + idx, pf);
       const T* xr = x + (int64_t)ld_stream(A.sCol + idx, pf) * K;
 #pragma unroll
       for (int i = 0; i < K; ++i) acc[i] += v * ld_keep(xr + i, pl);
     }
-    const int row = (int)A.sPerm[A.sSBs[sl] + lane];
     T* yr = Y + A.y_off + (int64_t)row * K;
 #pragma unroll
     for (int i = 0; i < K; ++i) store_y(yr + i, alpha, beta, acc[i]);
@@ -142,14 +175,35 @@ template <class T, int K>
 __global__ void __launch_bounds__(kBThreads)
 batched_kernel(int64_t ntiles, const BatchTile* __restrict__ tiles, const BatchMat* __restrict__ mats,
                const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta) {
+  // per tile: the matrix entry and the tile's row pointers (CSR) or slice
+  // metadata (SELL) are copied to shared memory once, then used by all warps
+  __shared__ int srst[kTileRowsMax + 1];
+  __shared__ int meta[4][kTileSlicesMax];
+  __shared__ __align__(16) unsigned char sAraw[sizeof(BatchMat)];
+  const BatchMat& A = *reinterpret_cast<const BatchMat*>(sAraw);
+  static_assert(sizeof(BatchMat) % 8 == 0, "BatchMat is copied as 8-byte words");
   for (int64_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
     const BatchTile t = tiles[ti];
-    const BatchMat& A = mats[t.mat];
-    if (A.mode == 0) {
-      if constexpr (K == 1) csr_k1<T>(A, t, X, Y, alpha, beta);
-      else csr_kn<T, K>(A, t, X, Y, alpha, beta);
+    __syncthreads();  // the previous tile is done with the shared copies
+    if (threadIdx.x < (int)(sizeof(BatchMat) / 8))
+      reinterpret_cast<uint64_t*>(sAraw)[threadIdx.x] =
+          reinterpret_cast<const uint64_t*>(mats + t.mat)[threadIdx.x];
+    __syncthreads();
+    if (A.mode == 0) {  // uniform over the CTA: the tile is shared
+      for (int i = threadIdx.x; i <= t.count; i += kBThreads) srst[i] = A.Rst[t.first + i];
+      __syncthreads();
+      if constexpr (K == 1) csr_k1<T>(A, t, srst, X, Y, alpha, beta);
+      else csr_kn<T, K>(A, t, srst, X, Y, alpha, beta);
     } else {
-      sell_kn<T, K>(A, t, X, Y, alpha, beta);
+      if (threadIdx.x < t.count) {
+        const int sl = t.first + threadIdx.x;
+        meta[0][threadIdx.x] = A.sBs[sl];
+        meta[1][threadIdx.x] = A.sCl[sl];
+        meta[2][threadIdx.x] = A.sCs[sl];
+        meta[3][threadIdx.x] = A.sSBs[sl];
+      }
+      __syncthreads();
+      sell_kn<T, K>(A, t, meta, X, Y, alpha, beta);
     }
   }
 }
@@ -299,7 +353,7 @@ int rvvla_batched_plan(const rvvla_crs* mats, int64_t count, int val_bytes, int 
       b.tpr = (k == 1) ? tpr : k;
       // tiles of whole rows: at most kTileWork products and at most 8 row
       // passes of the CTA
-      const int64_t max_rows = (int64_t)(kBThreads / b.tpr) * 8;
+      const int64_t max_rows = std::min<int64_t>((int64_t)(kBThreads / b.tpr) * 8, kTileRowsMax);
       int64_t r0 = 0;
       while (r0 < A.m) {
         int64_t r1 = r0, work = 0;
@@ -332,7 +386,7 @@ int rvvla_batched_plan(const rvvla_crs* mats, int64_t count, int val_bytes, int 
       int64_t q0 = 0;
       while (q0 < s.cnt_b) {
         int64_t q1 = q0, work = 0;
-        while (q1 < s.cnt_b && q1 - q0 < kBWarps * 4) {
+        while (q1 < s.cnt_b && q1 - q0 < kTileSlicesMax) {
           const int64_t wq = ((int64_t)Cl[(size_t)q1] + 1) * 32 * k;
           if (q1 > q0 && work + wq > 4 * kTileWork) break;
           work += wq;

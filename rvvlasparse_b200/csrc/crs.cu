@@ -19,11 +19,19 @@
 //      a second kernel adds carries in tile order (no float atomics, results
 //      are bitwise reproducible run to run).
 // The same kernels serve VNEC's L variant (merge-path CSR, vnec.cu).
+//
+// rvvla_crs_analyze picks the shared-memory-free warp-stream kernel instead
+// (crs_stream.cuh) for every matrix with nonzeros: directly when no row is
+// empty (plan kind 1), otherwise over the compacted non-empty rows with a map
+// back to the row ids and a separate beta pass over the empty rows (kind 2).
+// Plan kind 2 layout (int32): [mc, me, wrow[nw], Rst_c[mc+1], row_map[mc],
+// empty[me]] with plan_tiles = mc (nw follows from nz).
 #include <algorithm>
 
 #include "rvvla_internal.cuh"
 #include "crs_merge.cuh"
 #include "crs_stream.cuh"
+#include "scan.cuh"
 
 namespace rvvla {
 
@@ -43,6 +51,36 @@ __global__ void crs_stream_plan_kernel(int m, int nnz, const int* __restrict__ R
     wrow[t] = lo;
   }
   if (t < m && Rst[t + 1] == Rst[t]) atomicOr(any_empty, 1);
+}
+
+// kind 2: non-empty rows compacted (scan of the non-empty flags)
+__global__ void crs_nonempty_flags_kernel(int m, const int* __restrict__ Rst, int64_t* __restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) flag[i] = Rst[i + 1] > Rst[i] ? 1 : 0;
+}
+
+__global__ void crs_compact_kernel(int m, int nnz, const int* __restrict__ Rst, const int64_t* __restrict__ pos,
+                                   int* __restrict__ rst_c, int* __restrict__ row_map, int* __restrict__ empty) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    const int p = (int)pos[i];
+    if (Rst[i + 1] > Rst[i]) {
+      rst_c[p] = Rst[i];
+      row_map[p] = i;
+    } else {
+      empty[i - p] = i;
+    }
+  }
+  if (i == 0) rst_c[pos[m]] = nnz;
+}
+
+template <class X>
+__global__ void crs_empty_rows_kernel(int me, const int* __restrict__ empty, X* __restrict__ y, X beta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < me) {
+    const int r = empty[i];
+    y[r] = (beta == X(0)) ? X(0) : beta * y[r];
+  }
 }
 
 __global__ void merge_plan_kernel(int m, int nnz, const int* __restrict__ Rst, int tile_items, int ntiles,
@@ -91,21 +129,40 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
   int rc = crs_validate(A, x, y);
   if (rc) return rc;
   if (A->m == 0) return RVVLA_OK;
-  if (A->plan && A->plan_kind == 1) {  // no empty rows: shared-memory-free stream kernel
-    const int64_t nw = A->plan_tiles;
-    if (nw != (A->nz + kStreamE - 1) / kStreamE || A->nz == 0)
+  if (A->plan && (A->plan_kind == 1 || A->plan_kind == 2)) {  // shared-memory-free stream kernel
+    // kind 1: plan_tiles = warps, all rows; kind 2: plan_tiles = number of
+    // non-empty rows, the warps run over the compacted rows
+    const int64_t nw = (A->nz + kStreamE - 1) / kStreamE;
+    if (A->nz == 0 || (A->plan_kind == 1 && A->plan_tiles != nw) ||
+        (A->plan_kind == 2 && (A->plan_tiles <= 0 || A->plan_tiles > A->m)))
       return fail(RVVLA_ERR_INVALID_ARG, "crs: stream plan was built for a different matrix");
+    const int32_t* wrow = A->plan;
+    const int32_t* rst = A->Rst;
+    const int32_t* row_map = nullptr;
+    int mr = (int)A->m;
+    if (A->plan_kind == 2) {
+      const int mc = (int)A->plan_tiles, me = (int)(A->m - A->plan_tiles);
+      wrow = A->plan + 2;
+      rst = wrow + nw;
+      row_map = rst + mc + 1;
+      const int32_t* empty = row_map + mc;
+      mr = mc;
+      if (me > 0) {
+        crs_empty_rows_kernel<X><<<(unsigned)((me + 255) / 256), 256, 0, st>>>(me, empty, y, beta);
+        RVVLA_LAUNCHED("crs_empty_rows_kernel");
+      }
+    }
     Scratch sc;
     const size_t row_bytes = ((size_t)(2 * nw) * sizeof(int32_t) + 255) / 256 * 256;
     RVVLA_CUDA(sc.alloc(row_bytes + (size_t)(2 * nw) * sizeof(CT), st));
     int32_t* crow = sc.as<int32_t>();
     CT* cval = (CT*)(sc.as<char>() + row_bytes);
     crs_stream_kernel<V, X, Ac, CT><<<(unsigned)((nw * 32 + 255) / 256), 256, 0, st>>>(
-        (int)A->m, (int)A->nz, kStreamE, (int)nw, A->Rst, A->Col, (const V*)A->Val, x, y, alpha, beta, A->plan, crow,
-        cval);
+        mr, (int)A->nz, kStreamE, (int)nw, rst, A->Col, (const V*)A->Val, x, y, alpha, beta, wrow, crow, cval,
+        row_map);
     RVVLA_LAUNCHED("crs_stream_kernel");
     crs_stream_fixup_kernel<X, CT><<<(unsigned)((2 * nw + 255) / 256), 256, 0, st>>>((int)(2 * nw), crow, cval, y,
-                                                                                       alpha, beta);
+                                                                                       alpha, beta, row_map);
     RVVLA_LAUNCHED("crs_stream_fixup_kernel");
     return RVVLA_OK;
   }
@@ -143,7 +200,8 @@ extern "C" {
 
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype) {
   const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
-  return std::max<int64_t>(2 * (crs_tiles(m, nz, ipt) + 1), (nz + kStreamE - 1) / kStreamE);
+  const int64_t nw = (nz + kStreamE - 1) / kStreamE;
+  return std::max<int64_t>(2 * (crs_tiles(m, nz, ipt) + 1), 3 * m + nw + 3);
 }
 
 int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* plan_tiles, int32_t* plan_kind,
@@ -173,6 +231,34 @@ int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* pla
       *plan_kind = 1;
       return RVVLA_OK;
     }
+    // kind 2: compact the non-empty rows, then split the warps over them
+    Scratch s_flag, s_pos;
+    RVVLA_CUDA(s_flag.alloc((size_t)A->m * sizeof(int64_t), st));
+    RVVLA_CUDA(s_pos.alloc((size_t)(A->m + 1) * sizeof(int64_t), st));
+    const unsigned mb = (unsigned)((A->m + 255) / 256);
+    crs_nonempty_flags_kernel<<<mb, 256, 0, st>>>((int)A->m, A->Rst, s_flag.as<int64_t>());
+    RVVLA_LAUNCHED("crs_nonempty_flags_kernel");
+    int rc = exclusive_scan_i64(s_flag.as<int64_t>(), s_pos.as<int64_t>(), A->m, st);
+    if (rc) return rc;
+    int64_t mc = 0;
+    RVVLA_CUDA(cudaMemcpyAsync(&mc, s_pos.as<int64_t>() + A->m, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    RVVLA_CUDA(cudaStreamSynchronize(st));
+    const int64_t me = A->m - mc;
+    int32_t* wrow = plan + 2;
+    int32_t* rst_c = wrow + nw;
+    int32_t* row_map = rst_c + mc + 1;
+    int32_t* empty = row_map + mc;
+    crs_compact_kernel<<<mb, 256, 0, st>>>((int)A->m, (int)A->nz, A->Rst, s_pos.as<int64_t>(), rst_c, row_map, empty);
+    RVVLA_LAUNCHED("crs_compact_kernel");
+    crs_stream_plan_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>((int)mc, (int)A->nz, rst_c, kStreamE,
+                                                                         (int)nw, wrow, flag.as<int>());
+    RVVLA_LAUNCHED("crs_stream_plan_kernel");
+    const int32_t hdr[2] = {(int32_t)mc, (int32_t)me};
+    RVVLA_CUDA(cudaMemcpyAsync(plan, hdr, sizeof(hdr), cudaMemcpyHostToDevice, st));
+    RVVLA_CUDA(cudaStreamSynchronize(st));
+    *plan_tiles = mc;
+    *plan_kind = 2;
+    return RVVLA_OK;
   }
   *plan_tiles = crs_tiles(A->m, A->nz, ipt);
   *plan_kind = 0;

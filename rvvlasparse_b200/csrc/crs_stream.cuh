@@ -41,7 +41,8 @@ template <class V, class X, class Ac, class CT>
 __global__ void __launch_bounds__(256)
 crs_stream_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ Rst, const int* __restrict__ Col,
                   const V* __restrict__ Val, const X* __restrict__ x, X* __restrict__ y, X alpha, X beta,
-                  const int* __restrict__ wrow, int* __restrict__ carry_row, CT* __restrict__ carry_val) {
+                  const int* __restrict__ wrow, int* __restrict__ carry_row, CT* __restrict__ carry_val,
+                  const int* __restrict__ row_map) {
   const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const unsigned lane = threadIdx.x & 31;
   if (w >= nwarps) return;
@@ -105,7 +106,7 @@ crs_stream_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ Rst
             cfirst = acc_carry(acc);
             cfirst_row = r;
           } else {
-            write_row(y, r, alpha, beta, (X)acc_out(acc));
+            write_row(y, row_map ? row_map[r] : r, alpha, beta, (X)acc_out(acc));
           }
         }
         acc_zero(acc);
@@ -134,7 +135,7 @@ crs_stream_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ Rst
       }
       // a segment that ends before the chunk's last valid lane ends its row
       if (seg_end && (int)lane < last_valid && !(rel == 0 && first_piece_ends))
-        write_row(y, row, alpha, beta, (X)acc_out(s));
+        write_row(y, row_map ? row_map[row] : row, alpha, beta, (X)acc_out(s));
       // the segment at the last valid lane stays open
       const Ac tailv = acc_bcast(s, last_valid);
       const unsigned nh = __popc(heads & ((2u << last_valid) - 1u));
@@ -149,7 +150,7 @@ crs_stream_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ Rst
     int c1 = -1;
     CT v1 = CT(0);
     if (ends && !(open_is_first && first_open)) {
-      write_row(y, r, alpha, beta, (X)acc_out(acc));
+      write_row(y, row_map ? row_map[r] : r, alpha, beta, (X)acc_out(acc));
     } else if (open_is_first && first_open) {
       // one piece: the warp's first row is still open (or ends at ke)
       cfirst = acc_carry(acc);
@@ -169,7 +170,8 @@ crs_stream_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ Rst
 // row), so the run of equal rows is summed in warp order and written once.
 template <class X, class CT>
 __global__ void crs_stream_fixup_kernel(int nslots, const int* __restrict__ carry_row,
-                                        const CT* __restrict__ carry_val, X* __restrict__ y, X alpha, X beta) {
+                                        const CT* __restrict__ carry_val, X* __restrict__ y, X alpha, X beta,
+                                        const int* __restrict__ row_map) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nslots) return;
   const int r = carry_row[t];
@@ -185,7 +187,8 @@ __global__ void crs_stream_fixup_kernel(int nslots, const int* __restrict__ carr
     s += carry_val[u];
   }
   const X o = alpha * (X)s;
-  y[r] = (beta == X(0)) ? o : o + beta * y[r];
+  const int ro = row_map ? row_map[r] : r;
+  y[ro] = (beta == X(0)) ? o : o + beta * y[ro];
 }
 
 __global__ void crs_stream_plan_kernel(int m, int nnz, const int* __restrict__ Rst, int E, int nwarps,

@@ -214,6 +214,12 @@ __device__ __forceinline__ void write_first(X* y, int64_t r, CT v, X alpha, X be
 
 constexpr int bits_ce(int v) { return v ? 1 + bits_ce(v >> 1) : 0; }
 
+// Staging of a tile's values, columns and descriptor: straight into
+// registers; through a per-warp shared-memory ring filled by bulk copies; or
+// into registers one tile ahead (the next tile's loads overlap this tile's
+// gathers and reduction, at about twice the registers).
+constexpr int kC5Regs = 0, kC5Tma = 1, kC5Pipe = 2;
+
 // Shared-memory pipeline geometry of the bulk-copy kernel: per warp, STAGES
 // tiles of values + columns + descriptors (about 12 KB in flight per warp).
 constexpr int kC5Warps = 4;
@@ -234,7 +240,7 @@ struct C5Cfg {
 // bulk copies (values, columns, descriptors; L2 evict-first) and mbarrier
 // transaction counts; the warp gathers x for all SIGMA steps from registers
 // while later tiles are in flight.
-template <class V, class X, class Ac, class CT, int SIGMA, bool TMA>
+template <class V, class X, class Ac, class CT, int SIGMA, int MODE>
 __global__ void __launch_bounds__(kC5Warps * 32)
 csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, const uint32_t* __restrict__ colidx,
                  const V* __restrict__ vals, const uint32_t* __restrict__ tile_ptr,
@@ -264,6 +270,7 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, const uint32_t* __restrict__
     bulk_g2s(st + Cfg::VAL_B, colidx + t * Cfg::WS, Cfg::COL_B, &bars[s], pf);
     bulk_g2s(st + Cfg::VAL_B + Cfg::COL_B, desc + t * 32 * TDL, Cfg::DESC_B, &bars[s], pf);
   };
+  constexpr bool TMA = MODE == kC5Tma;
   if constexpr (TMA) {
     if (lane == 0) {
       for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
@@ -299,6 +306,22 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, const uint32_t* __restrict__
     cfirst = true;
   };
   using PT = decltype(Ops::prod(V(), X()));
+  // register variant: the columns, values and descriptor of tile t+1 are
+  // loaded before tile t gathers x, so the stream loads of the next tile are
+  // in flight during this tile's gathers and reduction
+  uint32_t cn[SIGMA];
+  V vn[SIGMA];
+  uint32_t dwn[TDL];
+  auto load_tile = [&](int64_t t) {
+    const int64_t base = t * (int64_t)Cfg::WS;
+#pragma unroll
+    for (int i = 0; i < SIGMA; ++i) cn[i] = ld_stream(colidx + base + i * 32 + lane, pf);
+#pragma unroll
+    for (int i = 0; i < SIGMA; ++i) vn[i] = ld_stream(vals + base + i * 32 + lane, pf);
+#pragma unroll
+    for (int d = 0; d < TDL; ++d) dwn[d] = ld_stream(desc + t * 32 * TDL + d * 32 + lane, pf);
+  };
+  if constexpr (MODE == kC5Pipe) load_tile(t0);
   for (int64_t t = t0; t < t1; ++t) {
     const int64_t it = t - t0;
     const int s = (int)(it % S);
@@ -336,15 +359,17 @@ csr5_spmv_kernel(int64_t nfull, int tiles_per_warp, const uint32_t* __restrict__
 #pragma unroll
       for (int i = 0; i < SIGMA; ++i) prod[i] = Ops::prod(v[i], ld_keep(x + c[i], pl));
     } else {
-      const int64_t base = t * (int64_t)Cfg::WS;
+      if constexpr (MODE == kC5Regs) load_tile(t);
       uint32_t c[SIGMA];
       V v[SIGMA];
 #pragma unroll
-      for (int i = 0; i < SIGMA; ++i) c[i] = ld_stream(colidx + base + i * 32 + lane, pf);
+      for (int i = 0; i < SIGMA; ++i) c[i] = cn[i];
 #pragma unroll
-      for (int i = 0; i < SIGMA; ++i) v[i] = ld_stream(vals + base + i * 32 + lane, pf);
+      for (int i = 0; i < SIGMA; ++i) v[i] = vn[i];
 #pragma unroll
-      for (int d = 0; d < TDL; ++d) dw[d] = ld_stream(desc + t * 32 * TDL + d * 32 + lane, pf);
+      for (int d = 0; d < TDL; ++d) dw[d] = dwn[d];
+      if constexpr (MODE == kC5Pipe)
+        if (t + 1 < t1) load_tile(t + 1);
 #pragma unroll
       for (int i = 0; i < SIGMA; ++i) prod[i] = Ops::prod(v[i], ld_keep(x + c[i], pl));
     }
@@ -597,16 +622,17 @@ __global__ void scale_kernel(int64_t m, X* __restrict__ y, X beta) {
   if (i < m) y[i] = (beta == X(0)) ? X(0) : beta * y[i];
 }
 
-// Staging variant of the templated kernel: direct register loads (default;
-// measured faster on B200: up to 28 resident warps per SM against 16 for the
-// per-warp shared-memory ring) or the bulk-copy pipeline
-// (RVVLA_CSR5_STAGING=tma, a tuning knob read once).
-bool csr5_register_variant() {
-  static const bool regs = [] {
+// Staging variant of the templated kernel (a tuning knob read once:
+// RVVLA_CSR5_STAGING=regs|tma|pipe).  Default: registers, which measured
+// faster on B200 than the shared-memory ring (up to 28 resident warps per SM
+// against 16).
+int csr5_staging() {
+  static const int mode = [] {
     const char* e = std::getenv("RVVLA_CSR5_STAGING");
-    return !(e && std::string(e) == "tma");
+    const std::string v = e ? e : "";
+    return v == "tma" ? kC5Tma : v == "pipe" ? kC5Pipe : kC5Regs;
   }();
-  return regs;
+  return mode;
 }
 
 int csr5_validate(const rvvla_csr5* A, const void* x, const void* y) {
@@ -627,21 +653,25 @@ int csr5_validate(const rvvla_csr5* A, const void* x, const void* y) {
 // 48: the SpMV launches one wave of exactly that many warps per SM (each warp
 // gets an equal share of tiles), so no partial second wave trails the grid.
 template <class V, class X, class Ac, class CT>
-int c5_resident_warps(int sigma, bool regs) {
-  static int cache[4][2] = {};
+int c5_resident_warps(int sigma, int mode) {
+  static int cache[4][3] = {};
   const int si = sigma / 8 - 1;
-  if (si < 0 || si > 3 || sigma % 8) return 48;
-  int& c = cache[si][regs ? 1 : 0];
+  if (si < 0 || si > 3 || sigma % 8 || mode < 0 || mode > 2) return 48;
+  int& c = cache[si][mode];
   if (c == 0) {
     int blocks = 0;
     cudaError_t e = cudaErrorInvalidValue;
     switch (sigma) {
-#define C5_OCC(S)                                                                                          \
-  case S:                                                                                                  \
-    e = regs ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, false>, \
-                                                            kC5Warps * 32, 0)                              \
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, true>,  \
-                                                            kC5Warps * 32, C5Cfg<V, S>::SMEM);             \
+#define C5_OCC(S)                                                                                             \
+  case S:                                                                                                     \
+    e = mode == kC5Tma                                                                                        \
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, kC5Tma>, \
+                                                            kC5Warps * 32, C5Cfg<V, S>::SMEM)                 \
+        : mode == kC5Pipe                                                                                     \
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, kC5Pipe>, \
+                                                            kC5Warps * 32, 0)                                 \
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, csr5_spmv_kernel<V, X, Ac, CT, S, kC5Regs>, \
+                                                            kC5Warps * 32, 0);                                \
     break;
       C5_OCC(8)
       C5_OCC(16)
@@ -672,8 +702,9 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
     // register-only kernel
     const bool aligned = ((uintptr_t)A->csr_value % 16 == 0) && ((uintptr_t)A->csr_column_index % 16 == 0) &&
                          ((uintptr_t)A->tile_descriptor % 16 == 0);
-    const bool use_regs = regs_only || csr5_register_variant();
-    const int per_sm = aligned ? c5_resident_warps<V, X, Ac, CT>(A->sigma, use_regs) : 48;
+    int mode = csr5_staging();
+    if (regs_only && mode == kC5Tma) mode = kC5Regs;
+    const int per_sm = aligned ? c5_resident_warps<V, X, Ac, CT>(A->sigma, mode) : 48;
     const int64_t want_warps = (int64_t)sm_count() * per_sm;
     int tpw = (int)std::max<int64_t>(1, (nfull + want_warps - 1) / want_warps);
     const int64_t nwarps = (nfull + tpw - 1) / tpw;
@@ -696,9 +727,10 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
     switch (aligned ? A->sigma : -1) {
 #define CSR5_CASE(S)                                                                                         \
   case S: {                                                                                                  \
-    auto k_ = csr5_spmv_kernel<V, X, Ac, CT, S, true>;                                                       \
-    if (use_regs) k_ = csr5_spmv_kernel<V, X, Ac, CT, S, false>;                                             \
-    const int smem_ = use_regs ? 0 : C5Cfg<V, S>::SMEM;                                                      \
+    auto k_ = csr5_spmv_kernel<V, X, Ac, CT, S, kC5Regs>;                                                    \
+    if (mode == kC5Tma) k_ = csr5_spmv_kernel<V, X, Ac, CT, S, kC5Tma>;                                      \
+    if (mode == kC5Pipe) k_ = csr5_spmv_kernel<V, X, Ac, CT, S, kC5Pipe>;                                    \
+    const int smem_ = mode == kC5Tma ? C5Cfg<V, S>::SMEM : 0;                                                \
     if (A->tile_desc_len != C5Cfg<V, S>::TDL || A->bit_y_offset != bits_ce(32 * S) || A->bit_seg_offset != 6)  \
       return fail(RVVLA_ERR_FORMAT, "csr5: descriptor widths do not match omega=32, sigma");                 \
     if (smem_ > 48 * 1024)                                                                                   \

@@ -168,21 +168,25 @@ __global__ void cvr_scale_kernel(int64_t m, X* __restrict__ y, X beta) {
   if (i < m) y[i] = (beta == X(0)) ? X(0) : y[i] * beta;
 }
 
-// A warp per CVR thread (lane = SIMD lane).  Vectors are fetched kCvrU at a
-// time (independent loads in flight), records are kept in a register window
-// of 32 (lane l holds record window_base + l) and reloaded only when the
-// window is used up.  A row belongs to one lane of one range, so each row of
-// y receives exactly one contribution: y was scaled by beta first and the
-// flush is a fire-and-forget atomic add (no read of y on the critical path,
-// and still deterministic).
-constexpr int kCvrU = 4;
+// A warp per CVR thread (lane = SIMD lane), kCvrU vectors per batch.  A
+// batch first issues all loads of its vectors (indices past the range are
+// clamped to its last vector and their products dropped), then marks the
+// records that fall in the batch in a per-warp table (vector in batch, lane)
+// -> row, then each lane walks the batch's vectors: flush into the marked row
+// (the record's position is the lane's first slot after the row), add the
+// product.  Records come from a 32-entry register window (lane l holds
+// record window_base + l) with the next window prefetched.  A row belongs to
+// one lane of one range, so each row of y receives exactly one contribution:
+// y was scaled by beta first and the flush is a fire-and-forget atomic add
+// (no read of y on the critical path, and still deterministic).
+constexpr int kCvrU = 8;
 
 template <class V, class X, class CT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 cvr_spmv_kernel(int64_t NT, int64_t nItems, int64_t nrec, const V* __restrict__ vals,
                 const uint32_t* __restrict__ cols, const int* __restrict__ rec, const int* __restrict__ wb,
                 const X* __restrict__ x, X* __restrict__ y, X alpha) {
-  __shared__ int s_row[8][kS];
+  __shared__ int s_row[8][kCvrU][kS];
   const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (t >= NT) return;
@@ -191,61 +195,91 @@ cvr_spmv_kernel(int64_t NT, int64_t nItems, int64_t nrec, const V* __restrict__ 
   const int64_t re = (t + 1 < NT) ? wb[(t + 1) * (kS + 2) + 1] : nrec;
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
   CT res = 0;
-  s_row[w][lane] = -1;
-  __syncwarp();
+#pragma unroll
+  for (int u = 0; u < kCvrU; ++u) s_row[w][u][lane] = -1;
+  // record window and its successor
+  auto avail = [&](int64_t base) { return (int)(re - base < 0 ? 0 : (re - base > kS ? kS : re - base)); };
   int64_t wbase = rb;
   int cons = 0;
-  int navail = (int)(re - wbase < 0 ? 0 : (re - wbase > kS ? kS : re - wbase));
+  int navail = avail(wbase);
   int my_pos = lane < navail ? rec[2 * (wbase + lane)] : INT_MAX;
   int my_row = lane < navail ? rec[2 * (wbase + lane) + 1] : -1;
-  // apply the records whose position falls before `limit`
-  auto apply = [&](int64_t limit) {
+  int nx_avail = avail(wbase + kS);
+  int nx_pos = lane < nx_avail ? rec[2 * (wbase + kS + lane)] : INT_MAX;
+  int nx_row = lane < nx_avail ? rec[2 * (wbase + kS + lane) + 1] : -1;
+  // mark the records before `limit` whose vector lies in [base, base + kCvrU)
+  auto mark = [&](int64_t limit, int64_t base) {
     for (;;) {
       if (cons == navail) {
         if (navail < kS) return;  // no records left in this range
         wbase += kS;
         cons = 0;
-        navail = (int)(re - wbase < 0 ? 0 : (re - wbase > kS ? kS : re - wbase));
+        navail = nx_avail;
+        my_pos = nx_pos;
+        my_row = nx_row;
         if (navail == 0) return;
-        my_pos = lane < navail ? rec[2 * (wbase + lane)] : INT_MAX;
-        my_row = lane < navail ? rec[2 * (wbase + lane) + 1] : -1;
+        nx_avail = avail(wbase + kS);
+        nx_pos = lane < nx_avail ? rec[2 * (wbase + kS + lane)] : INT_MAX;
+        nx_row = lane < nx_avail ? rec[2 * (wbase + kS + lane) + 1] : -1;
       }
       const bool take = lane >= cons && lane < navail && (int64_t)my_pos < limit;
       const unsigned mk = __ballot_sync(0xffffffffu, take);
-      if (!mk) return;
-      if (take) s_row[w][my_pos % kS] = my_row;
-      __syncwarp();
-      const int r = s_row[w][lane];
-      if (r >= 0) {
-        if (res != CT(0)) atomicAdd(y + r, alpha * (X)res);
-        res = 0;
-        s_row[w][lane] = -1;
+      if (take) {
+        const int64_t u = (int64_t)my_pos / kS - base;
+        if (u >= 0 && u < kCvrU) s_row[w][u][my_pos % kS] = my_row;
       }
-      __syncwarp();
       cons += __popc(mk);
       if (cons < navail) return;  // stopped at a record past the limit
     }
   };
-  for (int64_t v = vb; v < ve; v += kCvrU) {
+  auto flush_batch = [&](int nu, const CT* p) {
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kCvrU; ++u) {
+      const int r = s_row[w][u][lane];
+      if (r >= 0) {
+        if (res != CT(0)) atomicAdd(y + r, alpha * (X)res);
+        res = 0;
+        s_row[w][u][lane] = -1;
+      }
+      if (u < nu) res += p[u];
+    }
+    __syncwarp();
+  };
+  int64_t v = vb;
+  for (; v < ve; v += kCvrU) {
+    uint32_t c[kCvrU];
+    V a[kCvrU];
+    X xv[kCvrU];
+#pragma unroll
+    for (int u = 0; u < kCvrU; ++u) c[u] = ld_stream(cols + min(v + u, ve - 1) * kS + lane, pf);
+#pragma unroll
+    for (int u = 0; u < kCvrU; ++u) a[u] = ld_stream(vals + min(v + u, ve - 1) * kS + lane, pf);
+#pragma unroll
+    for (int u = 0; u < kCvrU; ++u) xv[u] = ld_keep(x + c[u], pl);
+    mark((v + kCvrU) * kS, v);
     CT p[kCvrU];
 #pragma unroll
-    for (int u = 0; u < kCvrU; ++u) {
-      p[u] = 0;
-      if (v + u < ve) {
-        const int64_t k = (v + u) * kS + lane;
-        const uint32_t c = ld_stream(cols + k, pf);
-        p[u] = (CT)vmul(ld_stream(vals + k, pf), ld_keep(x + c, pl));
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kCvrU; ++u) {
-      if (v + u < ve) {
-        apply((v + u) * kS + kS);
-        res += p[u];
-      }
-    }
+    for (int u = 0; u < kCvrU; ++u) p[u] = (CT)vmul(a[u], xv[u]);
+    flush_batch(ve - v < kCvrU ? (int)(ve - v) : kCvrU, p);
   }
-  apply(INT64_MAX);
+  // records left: the range-end flushes at vector ve (one batch suffices for
+  // well-formed records; later ones take further batches)
+  CT none[kCvrU];
+#pragma unroll
+  for (int u = 0; u < kCvrU; ++u) none[u] = 0;
+  for (int guard = 0; guard < 64; ++guard) {
+    if (cons == navail && navail < kS) break;
+    const int64_t p0 = __shfl_sync(0xffffffffu, my_pos, cons < kS ? cons : 0);
+    if (cons == navail) {  // window used up: reload through mark
+      mark(v * kS, v);
+      continue;
+    }
+    v = p0 / kS > v ? p0 / kS : v;
+    mark((v + kCvrU) * kS, v);
+    flush_batch(0, none);
+    v += kCvrU;
+  }
   if (t + 1 == NT) {  // the last range's tail rows
     const int r = wb[t * (kS + 2) + 2 + lane];
     if (res != CT(0)) atomicAdd(y + r, alpha * (X)res);
@@ -283,10 +317,12 @@ int cvr_build_impl(const rvvla_crs* src, int vb, int64_t NT, rvvla_cvr_owned* ou
   if (vb != 8 && vb != 4 && vb != 2) return fail(RVVLA_ERR_INVALID_ARG, "cvr_build: val_bytes must be 8, 4 or 2");
   const int64_t m = src->m, nnz = src->nz;
   if (m < 0 || nnz < 0 || src->n < 0) return fail(RVVLA_ERR_INVALID_ARG, "cvr_build: bad sizes");
-  // ranges of ~32K nonzeros: smaller ranges drain their lanes unevenly and
-  // pad the vectors (2K nonzeros per range triples the stored items on a
-  // power-law matrix, 32K adds ~3 %)
-  if (NT <= 0) NT = std::max<int64_t>(1, (nnz + 32767) / 32768);
+  // ranges of ~16K nonzeros: smaller ranges drain their lanes unevenly and
+  // pad the vectors (4K nonzeros per range double the stored items of a
+  // power-law matrix, 8K add ~40 %, 16K ~10 %, 32K ~2 %), larger ones leave
+  // too few warps to hide the memory latency (rounding the count to whole
+  // waves of resident warps measured no faster)
+  if (NT <= 0) NT = std::max<int64_t>(1, (nnz + 16383) / 16384);
   if (nnz >= INT32_MAX / 2 || m >= INT32_MAX) return fail(RVVLA_ERR_TOO_LARGE, "cvr_build: sizes beyond int32 records");
   rvvla_cvr& h = out->h;
   h.numRows = m; h.numCols = src->n; h.SIMD_LEN = kS; h.Nthreads = (int32_t)NT; h.Nthreads_avail = (int32_t)NT;

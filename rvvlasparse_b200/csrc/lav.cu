@@ -63,25 +63,93 @@ lav_segment_kernel(int64_t s, int64_t L, int64_t cc, const int* __restrict__ co,
   y[r] += alpha * (X)acc;
 }
 
-// All segments in one pass (L divides 32): lane (c, j) of a warp owns slot j
-// of chunk c, i.e. row row_order[c*L + j].  In every segment lane (c, i)
-// sums its steps for the row the segment placed at lane i, and the slot
-// owner takes that sum from lane lane_of_slot[(s, c, j)] with a shuffle, so a
-// row's segment sums are added in registers in segment order and y is
-// read-modified-written once (after the sparse part has applied beta).
+// All segments in one pass (L divides 32).  Blocks [0, nlong) take the
+// long chunks [0, nlong), one CTA each: thread (g, i) sums every G-th step
+// (G = 256 / L) of lane i, the groups' partial sums are added in group
+// order through shared memory, and thread j < L owns slot j.  The remaining
+// blocks give lane (c, j) of a warp slot j of chunk c >= nlong, i.e. row
+// row_order[c*L + j]: in every segment lane (c, i) sums its steps for the row
+// the segment placed at lane i, and the slot owner takes that sum from lane
+// lane_of_slot[(s, c, j)] with a shuffle.  Either way a row's segment sums
+// are added in segment order and y is read-modified-written once (after the
+// sparse part has applied beta).  Chunks are cut from rows sorted by dense
+// count, so the long chunks lead and their CTAs start first.
+//
+// Loads: each thread issues all loads of 4 steps before using any (steps
+// past the chunk's end are clamped to its last step, which holds L slots,
+// and dropped); x is gathered at min(col, n-1) so that padding slots need
+// no mask test first, and a product counts only where the step is active
+// (every lane before fe, the first mask[q] lanes after it).
+template <class V, class X, class CT, int L>
+__device__ __forceinline__ CT lav_steps(int q, int qend, int qstride, int fe, int i, int64_t base, int64_t nmax,
+                                        const uint16_t* __restrict__ mk, const V* __restrict__ val,
+                                        const uint32_t* __restrict__ col, const X* __restrict__ x, uint64_t pf,
+                                        uint64_t pl) {
+  CT part = 0;
+  for (; q < qend; q += 4 * qstride) {
+    int64_t e[4];
+    uint32_t ci[4];
+    V vv[4];
+    X xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) e[u] = base + min(q + u * qstride, qend - 1);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ci[u] = ld_stream(col + e[u] * L + i, pf);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) vv[u] = ld_stream(val + e[u] * L + i, pf);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xv[u] = ld_keep(x + min((int64_t)ci[u], nmax), pl);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int qq = q + u * qstride;
+      if (qq < qend && (qq < fe || i < (int)mk[e[u]])) part += (CT)vmul(vv[u], xv[u]);
+    }
+  }
+  return part;
+}
+
 template <class V, class X, class CT, int L>
 __global__ void __launch_bounds__(256)
-lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, const int* __restrict__ co, const int* __restrict__ cf,
-                 const uint64_t* __restrict__ sp, const uint16_t* __restrict__ mk, const V* __restrict__ val,
-                 const uint32_t* __restrict__ col, const uint8_t* __restrict__ los,
+lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, int64_t n, int64_t nlong, const int* __restrict__ co,
+                 const int* __restrict__ cf, const uint64_t* __restrict__ sp, const uint16_t* __restrict__ mk,
+                 const V* __restrict__ val, const uint32_t* __restrict__ col, const uint8_t* __restrict__ los,
                  const uint32_t* __restrict__ row_order, const X* __restrict__ x, X* __restrict__ y, X alpha) {
   static_assert(32 % L == 0, "a chunk must not straddle warps");
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int G = 256 / L;
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+  const int64_t nmax = n > 0 ? n - 1 : 0;
+  if ((int64_t)blockIdx.x < nlong) {
+    __shared__ CT red[256];
+    const int64_t c = blockIdx.x;
+    const int g = threadIdx.x / L, i = threadIdx.x % L;
+    CT acc = 0;
+    for (int64_t s = 0; s < nseg; ++s) {
+      const int64_t sh = (cc + 1) * s;
+      const int st = co[sh + c], en = co[sh + c + 1];
+      if (st >= en) continue;  // the same for the whole block
+      const int fe = cf[s * cc + c];
+      red[threadIdx.x] = lav_steps<V, X, CT, L>(st + g, en, G, fe, i, (int64_t)sp[s], nmax, mk, val, col, x, pf, pl);
+      __syncthreads();
+      if (threadIdx.x < L) {
+        const int src = los[(s * cc + c) * L + threadIdx.x];
+        CT segsum = 0;
+        for (int gg = 0; gg < G; ++gg) segsum += red[gg * L + src];
+        acc += segsum;
+      }
+      __syncthreads();
+    }
+    const int64_t gs = c * L + threadIdx.x;
+    if (threadIdx.x < L && gs < m) {
+      const uint32_t r = row_order[gs];
+      y[r] += alpha * (X)acc;
+    }
+    return;
+  }
+  const int64_t gid = nlong * L + ((int64_t)blockIdx.x - nlong) * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int64_t c = gid / L;
   const int i = (int)(gid % L);
   const bool live = c < cc;
-  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
   CT acc = 0;
   for (int64_t s = 0; s < nseg; ++s) {
     CT part = 0;
@@ -90,33 +158,8 @@ lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, const int* __restrict__ co
       const int64_t sh = (cc + 1) * s;
       const int st = co[sh + c], en = co[sh + c + 1];
       if (st < en) {
-        const int fe = cf[s * cc + c];
-        const int64_t base = (int64_t)sp[s];
         src = los[(s * cc + c) * L + i];
-        // steps four at a time (independent loads in flight); a step is
-        // active for every lane before fe, and for the first mask[q] lanes
-        // after it
-        for (int q0 = st; q0 < en; q0 += 4) {
-          bool act[4];
-          uint32_t ci[4];
-          V vv[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int q = q0 + u;
-            act[u] = q < en && (q < fe || i < (int)mk[base + q]);
-          }
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (act[u]) {
-              const int64_t e = (base + q0 + u) * L + i;
-              ci[u] = ld_stream(col + e, pf);
-              vv[u] = ld_stream(val + e, pf);
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < 4; ++u)
-            if (act[u]) part += (CT)vmul(vv[u], ld_keep(x + ci[u], pl));
-        }
+        part = lav_steps<V, X, CT, L>(st, en, 1, cf[s * cc + c], i, (int64_t)sp[s], nmax, mk, val, col, x, pf, pl);
       }
     }
     acc += __shfl_sync(0xffffffffu, part, (lane & ~(L - 1)) + src);
@@ -127,6 +170,8 @@ lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, const int* __restrict__ co
     y[r] += alpha * (X)acc;
   }
 }
+
+constexpr int64_t kLavLongSteps = 128;
 
 template <class T>
 int upload(const std::vector<T>& v, T** dst, cudaStream_t st) {
@@ -165,6 +210,14 @@ int lav_build_typed(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen
   h.col_id = out->col_id;
   h.row_order = out->row_order;
   h.lane_of_slot = out->lane_of_slot;
+  // the leading chunks up to the last one of >= kLavLongSteps steps (summed
+  // over the segments) get a thread block each
+  h.long_chunks = 0;
+  for (int64_t c = 0; c < H.cc; ++c) {
+    int64_t steps = 0;
+    for (int64_t s = 0; s < H.nseg; ++s) steps += H.co[(size_t)((H.cc + 1) * s + c + 1)] - H.co[(size_t)((H.cc + 1) * s + c)];
+    if (steps >= kLavLongSteps) h.long_chunks = c + 1;
+  }
   h.sparse_part.m = m; h.sparse_part.n = src->n; h.sparse_part.nz = (int64_t)H.sCol.size();
   h.sparse_part.Rst = out->sp_Rst; h.sparse_part.Col = out->sp_Col; h.sparse_part.Val = out->sp_Val;
   h.sparse_part.plan = nullptr; h.sparse_part.plan_tiles = 0; h.sparse_part.plan_kind = 0;
@@ -185,12 +238,18 @@ int lav_spmv_impl(const rvvla_lav* A, X alpha, const X* x, X beta, X* y, cudaStr
   const int64_t threads = A->chunk_count * A->SIMD_Lanes;
   if (A->segment_count == 0) return RVVLA_OK;
   if (A->row_order && A->lane_of_slot && A->SIMD_Lanes <= 32 && 32 % A->SIMD_Lanes == 0) {
-    const int64_t total = (threads + 31) / 32 * 32;  // whole warps: every lane takes part in the shuffles
-    const unsigned blocks = (unsigned)((total + 255) / 256);
+    // long chunks: a multiple of the chunks per warp, so that the rest
+    // starts on a warp boundary
+    const int64_t cpw = 32 / A->SIMD_Lanes;
+    const int64_t nlong = std::min(A->chunk_count, std::max<int64_t>(A->long_chunks, 0) + cpw - 1) / cpw * cpw;
+    const int64_t rest = (A->chunk_count - nlong) * A->SIMD_Lanes;
+    const int64_t total = (rest + 31) / 32 * 32;  // whole warps: every lane takes part in the shuffles
+    const unsigned blocks = (unsigned)(nlong + (total + 255) / 256);
     switch (A->SIMD_Lanes) {
 #define LAV_FUSED(LN)                                                                                          \
   case LN:                                                                                                     \
-    lav_fused_kernel<V, X, CT, LN><<<blocks, 256, 0, st>>>(A->segment_count, A->chunk_count, A->m,             \
+    lav_fused_kernel<V, X, CT, LN><<<blocks, 256, 0, st>>>(A->segment_count, A->chunk_count, A->m, A->n,       \
+                                                          nlong,                                              \
                                                           A->chunk_offsets, A->chunk_offsets_full_mask,       \
                                                           A->segment_ptr, A->mask, (const V*)A->val,          \
                                                           A->col_id, A->lane_of_slot, A->row_order, x, y,     \

@@ -355,7 +355,8 @@ class spMtxLAV(_GpuFormat):
     """``spMtxLAV<ValT>`` (include/LAV.h:11-31); ``sparse_part`` is an
     :class:`spMtxCRS` on the same device."""
 
-    SCALARS = ("SIMD_Lanes", "m", "n", "nz", "segment_count", "chunk_count", "segment_len", "n_steps")
+    SCALARS = ("SIMD_Lanes", "m", "n", "nz", "segment_count", "chunk_count", "segment_len", "n_steps",
+               "long_chunks")
     ARRAYS = {"chunk_offsets": torch.int32, "chunk_offsets_full_mask": torch.int32, "segment_ptr": torch.int64,
               "out_order": torch.int32, "mask": torch.int16, "val": None, "col_id": torch.int32,
               "row_order": torch.int32, "lane_of_slot": torch.uint8}

@@ -5,6 +5,8 @@ long-double CSR oracle; mixed (fp32 values and x, compensated fp32 sums)
 <= 1e-6 against the fp64 oracle on the fp64 matrix; the HCSR builder equals
 the reference's convert<T, spMtxHCSR, false> bit for bit.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 import torch
@@ -246,7 +248,45 @@ def test_crs_stream_plan_selected_and_edge_rows():
     assert O.normwise_relerr(y32, yref) < 1e-5
 
 
-def test_crs_empty_rows_use_merge_plan(g):
+def test_crs_plan_kinds_and_merge_path(g):
+    """Matrices with empty rows get the stream kernel over the compacted
+    non-empty rows (kind 2), others the plain stream (kind 1); a descriptor
+    without a plan runs the merge-path kernel.  All agree with the oracle."""
     A = gpu_crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
     has_empty = np.any(np.diff(g["Rst"]) == 0)
-    assert A.plan(0)[2] == (0 if has_empty else 1)
+    assert A.plan(0)[2] == (2 if has_empty else 1)
+    tol = tol_for(g["Val"].dtype)
+    yref = O.crs_spmv_ld(O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"]), g["alpha"], g["x"], g["beta"], g["y0"])
+    assert O.normwise_relerr(run(A, g["alpha"], g["x"], g["beta"], g["y0"]), yref) < tol
+    lib = R.load()
+    d = A.desc()  # no plan: merge path
+    y = dev(g["y0"])
+    fn = lib.rvvla_crs_spmv_f64 if g["Val"].dtype == np.float64 else lib.rvvla_crs_spmv_f32
+    assert fn(C.byref(d), g["alpha"], dev(g["x"]).data_ptr(), g["beta"], y.data_ptr(),
+              torch.cuda.current_stream().cuda_stream) == 0
+    torch.cuda.synchronize()
+    assert O.normwise_relerr(y.cpu().numpy(), yref) < tol
+
+
+@pytest.mark.parametrize("empty_frac", [0.05, 0.6, 0.99])
+def test_crs_stream_over_nonempty_rows(empty_frac):
+    """Kind 2 with few, many and almost all rows empty, fp64 and fp32, beta
+    on the empty rows included; NaN in y must not survive beta = 0."""
+    rng = np.random.default_rng(int(empty_frac * 100))
+    m, n = 50000, 30000
+    lens = rng.poisson(12, m)
+    lens[rng.random(m) < empty_frac] = 0
+    Rst = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    Col = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    Val = rng.uniform(-1, 1, len(Col))
+    A = gpu_crs(m, n, Rst, Col, Val)
+    assert A.plan(0)[2] == 2
+    x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, m)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 0.5, x, 2.0, y0)
+    assert O.normwise_relerr(run(A, 0.5, x, 2.0, y0), yref) < 1e-12
+    A32 = gpu_crs(m, n, Rst, Col, Val.astype(np.float32))
+    y32 = run(A32, 0.5, x.astype(np.float32), 2.0, y0.astype(np.float32))
+    assert O.normwise_relerr(y32, yref) < 1e-5
+    y0n = np.full(m, np.nan)
+    yz = run(A, 1.0, x, 0.0, y0n)
+    assert np.all(np.isfinite(yz))

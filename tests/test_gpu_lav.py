@@ -93,3 +93,18 @@ def test_lav_large(dt):
     y = run(V, 1.0, x, 0.5, y0)
     yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.5, y0)
     assert O.normwise_relerr(y, yref) < tol_for(dt)
+
+
+@pytest.mark.parametrize("lanes,seglen", [(8, 1 << 18), (8, 4096), (32, 50000), (1, 1 << 18), (4, 9000)])
+def test_lav_long_chunks(lanes, seglen):
+    # rows of up to 4096 nonzeros: the leading chunks run as one thread block
+    # each; the result must not depend on how many chunks take that path
+    m, n, Rst, Col, Val = W.powerlaw(1 << 18, seed=11)
+    V = build(m, n, Rst, Col, Val, lanes, 0.2, seglen)
+    assert 0 < V.long_chunks < V.chunk_count
+    x, y0 = W.vector(n, 2), W.vector(m, 3)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 0.75, x, -0.5, y0)
+    for nl in (V.long_chunks, 0, 1, V.chunk_count - 1, V.chunk_count):
+        V.long_chunks = nl
+        y = run(V, 0.75, x, -0.5, y0)
+        assert O.normwise_relerr(y, yref) < tol_for(np.float64), nl
