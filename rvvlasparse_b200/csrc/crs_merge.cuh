@@ -30,6 +30,14 @@ __device__ __forceinline__ CompF32 acc_shfl_up(CompF32 a, int d) {
   r.c = __shfl_up_sync(0xffffffffu, a.c, d);
   return r;
 }
+__device__ __forceinline__ double acc_shfl_xor(double a, int d) { return __shfl_xor_sync(0xffffffffu, a, d); }
+__device__ __forceinline__ float acc_shfl_xor(float a, int d) { return __shfl_xor_sync(0xffffffffu, a, d); }
+__device__ __forceinline__ CompF32 acc_shfl_xor(CompF32 a, int d) {
+  CompF32 r;
+  r.s = __shfl_xor_sync(0xffffffffu, a.s, d);
+  r.c = __shfl_xor_sync(0xffffffffu, a.c, d);
+  return r;
+}
 __device__ __forceinline__ double acc_bcast(double a, int l) { return __shfl_sync(0xffffffffu, a, l); }
 __device__ __forceinline__ float acc_bcast(float a, int l) { return __shfl_sync(0xffffffffu, a, l); }
 __device__ __forceinline__ CompF32 acc_bcast(CompF32 a, int l) {
