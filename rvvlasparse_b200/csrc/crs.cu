@@ -20,18 +20,25 @@
 //      are bitwise reproducible run to run).
 // The same kernels serve VNEC's L variant (merge-path CSR, vnec.cu).
 //
-// rvvla_crs_analyze picks the shared-memory-free warp-stream kernel instead
-// (crs_stream.cuh) for every matrix with nonzeros: directly when no row is
-// empty (plan kind 1), otherwise over the compacted non-empty rows with a map
-// back to the row ids and a separate beta pass over the empty rows (kind 2).
-// Plan kind 2 layout (int32): [mc, me, wrow[nw], Rst_c[mc+1], row_map[mc],
-// empty[me]] with plan_tiles = mc (nw follows from nz).
+// rvvla_crs_analyze picks the shared-memory-free lane-run kernel instead
+// (crs_run.cuh; the warp-stream kernel of crs_stream.cuh on the same plan
+// with RVVLA_CRS_KERNEL=stream) for every matrix with nonzeros: directly when
+// no row is empty (plan kind 1), otherwise over the compacted non-empty rows
+// with a map back to the row ids and a separate beta pass over the empty rows
+// (kind 2).  Plan layouts (int32): kind 1 [wrow[nw], bits]; kind 2 [mc, me,
+// wrow[nw], Rst_c[mc+1], row_map[mc], empty[me], bits] with plan_tiles = mc
+// (nw follows from nz); bits = the row-start bitmap over the nonzeros,
+// (nz + 31) / 32 words.
 #include <algorithm>
 
 #include "rvvla_internal.cuh"
 #include "crs_merge.cuh"
+#include "crs_run.cuh"
 #include "crs_stream.cuh"
 #include "scan.cuh"
+
+#include <cstdlib>
+#include <string>
 
 namespace rvvla {
 
@@ -99,6 +106,15 @@ __global__ void merge_plan_kernel(int m, int nnz, const int* __restrict__ Rst, i
   plan[2 * t + 1] = diag - lo;
 }
 
+// The kernel for plan kinds 1 and 2 (a tuning knob read once).
+bool crs_use_stream_kernel() {
+  static const bool stream = [] {
+    const char* e = std::getenv("RVVLA_CRS_KERNEL");
+    return e && std::string(e) == "stream";
+  }();
+  return stream;
+}
+
 int64_t crs_tiles(int64_t m, int64_t nz, int ipt) {
   const int64_t tile = (int64_t)kMergeBlock * ipt;
   return (m + nz + tile - 1) / tile;
@@ -139,6 +155,7 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
     const int32_t* wrow = A->plan;
     const int32_t* rst = A->Rst;
     const int32_t* row_map = nullptr;
+    const uint32_t* bits = reinterpret_cast<const uint32_t*>(A->plan + nw);
     int mr = (int)A->m;
     if (A->plan_kind == 2) {
       const int mc = (int)A->plan_tiles, me = (int)(A->m - A->plan_tiles);
@@ -146,6 +163,7 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
       rst = wrow + nw;
       row_map = rst + mc + 1;
       const int32_t* empty = row_map + mc;
+      bits = reinterpret_cast<const uint32_t*>(empty + me);
       mr = mc;
       if (me > 0) {
         crs_empty_rows_kernel<X><<<(unsigned)((me + 255) / 256), 256, 0, st>>>(me, empty, y, beta);
@@ -157,10 +175,24 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
     RVVLA_CUDA(sc.alloc(row_bytes + (size_t)(2 * nw) * sizeof(CT), st));
     int32_t* crow = sc.as<int32_t>();
     CT* cval = (CT*)(sc.as<char>() + row_bytes);
-    crs_stream_kernel<V, X, Ac, CT><<<(unsigned)((nw * 32 + 255) / 256), 256, 0, st>>>(
-        mr, (int)A->nz, kStreamE, (int)nw, rst, A->Col, (const V*)A->Val, x, y, alpha, beta, wrow, crow, cval,
-        row_map);
-    RVVLA_LAUNCHED("crs_stream_kernel");
+    const unsigned blocks = (unsigned)((nw * 32 + 255) / 256);
+    if (crs_use_stream_kernel()) {
+      crs_stream_kernel<V, X, Ac, CT><<<blocks, 256, 0, st>>>(mr, (int)A->nz, kStreamE, (int)nw, rst, A->Col,
+                                                              (const V*)A->Val, x, y, alpha, beta, wrow, crow, cval,
+                                                              row_map);
+      RVVLA_LAUNCHED("crs_stream_kernel");
+    } else {
+      const bool vec = (uintptr_t)A->Col % 16 == 0 && (uintptr_t)A->Val % 16 == 0;
+      if (vec)
+        crs_run_kernel<V, X, Ac, CT, true><<<blocks, 256, 0, st>>>(mr, (int)A->nz, kStreamE, (int)nw, rst, bits,
+                                                                   A->Col, (const V*)A->Val, x, y, alpha, beta, wrow,
+                                                                   crow, cval, row_map);
+      else
+        crs_run_kernel<V, X, Ac, CT, false><<<blocks, 256, 0, st>>>(mr, (int)A->nz, kStreamE, (int)nw, rst, bits,
+                                                                    A->Col, (const V*)A->Val, x, y, alpha, beta, wrow,
+                                                                    crow, cval, row_map);
+      RVVLA_LAUNCHED("crs_run_kernel");
+    }
     crs_stream_fixup_kernel<X, CT><<<(unsigned)((2 * nw + 255) / 256), 256, 0, st>>>((int)(2 * nw), crow, cval, y,
                                                                                        alpha, beta, row_map);
     RVVLA_LAUNCHED("crs_stream_fixup_kernel");
@@ -201,7 +233,7 @@ extern "C" {
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype) {
   const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
   const int64_t nw = (nz + kStreamE - 1) / kStreamE;
-  return std::max<int64_t>(2 * (crs_tiles(m, nz, ipt) + 1), 3 * m + nw + 3);
+  return std::max<int64_t>(2 * (crs_tiles(m, nz, ipt) + 1), 3 * m + nw + 3 + (nz + 31) / 32);
 }
 
 int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* plan_tiles, int32_t* plan_kind,
@@ -227,6 +259,11 @@ int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* pla
     RVVLA_CUDA(cudaMemcpyAsync(&any_empty, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     RVVLA_CUDA(cudaStreamSynchronize(st));
     if (!any_empty) {
+      uint32_t* bits = reinterpret_cast<uint32_t*>(plan + nw);
+      RVVLA_CUDA(cudaMemsetAsync(bits, 0, (size_t)((A->nz + 31) / 32) * sizeof(uint32_t), st));
+      crs_run_bits_kernel<<<(unsigned)((A->m + 255) / 256), 256, 0, st>>>((int)A->m, A->Rst, bits);
+      RVVLA_LAUNCHED("crs_run_bits_kernel");
+      RVVLA_CUDA(cudaStreamSynchronize(st));
       *plan_tiles = nw;
       *plan_kind = 1;
       return RVVLA_OK;
@@ -253,6 +290,12 @@ int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* pla
     crs_stream_plan_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>((int)mc, (int)A->nz, rst_c, kStreamE,
                                                                          (int)nw, wrow, flag.as<int>());
     RVVLA_LAUNCHED("crs_stream_plan_kernel");
+    uint32_t* bits = reinterpret_cast<uint32_t*>(empty + me);
+    RVVLA_CUDA(cudaMemsetAsync(bits, 0, (size_t)((A->nz + 31) / 32) * sizeof(uint32_t), st));
+    if (mc > 0) {
+      crs_run_bits_kernel<<<(unsigned)((mc + 255) / 256), 256, 0, st>>>((int)mc, rst_c, bits);
+      RVVLA_LAUNCHED("crs_run_bits_kernel");
+    }
     const int32_t hdr[2] = {(int32_t)mc, (int32_t)me};
     RVVLA_CUDA(cudaMemcpyAsync(plan, hdr, sizeof(hdr), cudaMemcpyHostToDevice, st));
     RVVLA_CUDA(cudaStreamSynchronize(st));
