@@ -312,6 +312,12 @@ typedef struct rvvla_vnec {
   const int32_t* reorder_col;
   const void* reorder_nnz;
   int64_t ntasks, nreorder;
+  /* Optional (not in the reference class): the rvvla_crs_analyze plan of the
+   * source CRS for the L variant (NULL = merge path over the VNEC threads'
+   * coordinates). */
+  const int32_t* plan;
+  int64_t plan_tiles;
+  int32_t plan_kind;
 } rvvla_vnec;
 
 typedef struct rvvla_vnec_owned {
@@ -323,6 +329,7 @@ typedef struct rvvla_vnec_owned {
   void* val_align;
   int32_t *tasks, *task_start, *task_end, *spvv_len, *row_begin, *row_end, *reorder_col;
   void* reorder_nnz;
+  int32_t* plan;
 } rvvla_vnec_owned;
 
 /* spMtxVNEC(const spMtxCRS&) (include/VNEC.h:200-227): partition, x

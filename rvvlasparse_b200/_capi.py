@@ -57,7 +57,7 @@ class rvvla_sell_owned(C.Structure):
 
 VNEC_ARRAYS = ("ptr", "indices", "val", "thread_coord_start", "thread_coord_end", "ecr_indices", "NEC_NUM",
                "use_x_ptr", "use_x_indices", "v_row_ptr", "col_start", "val_align", "tasks", "task_start",
-               "task_end", "spvv_len", "row_begin", "row_end", "reorder_col", "reorder_nnz")
+               "task_end", "spvv_len", "row_begin", "row_end", "reorder_col", "reorder_nnz", "plan")
 
 
 class rvvla_transpose(C.Structure):
@@ -99,7 +99,7 @@ class rvvla_vnec(C.Structure):
                 ("use_x_ptr", vp), ("use_x_indices", vp), ("v_row_ptr", vp), ("col_start", vp),
                 ("val_align", vp), ("ngroups", i64), ("tasks", vp), ("task_start", vp), ("task_end", vp),
                 ("spvv_len", vp), ("row_begin", vp), ("row_end", vp), ("reorder_col", vp), ("reorder_nnz", vp),
-                ("ntasks", i64), ("nreorder", i64)]
+                ("ntasks", i64), ("nreorder", i64), ("plan", vp), ("plan_tiles", i64), ("plan_kind", i32)]
 
 
 class rvvla_vnec_owned(C.Structure):

@@ -1,10 +1,12 @@
 // vnec.cu — spMtxVNEC on sm_100a (variants S, D, L of
 // src/rvv/spmv_mtx_vnec.cpp:78-586; selection include/VNEC.h:218-226).
 //
-//   L (merge-path CSR, :448-586): the merge-path kernels of crs.cu with the
-//     structure's thread coordinates as tile boundaries (one CTA per VNEC
-//     thread) when a thread holds at most one tile of items, else a fresh
-//     merge-path split;
+//   L (merge-path CSR, :448-586): the builder analyses the source CRS and the
+//     SpMV runs the CRS lane-run kernel of crs.cu on that plan (the product is
+//     the CRS one; the reference's merge path is only its CPU split); without
+//     a plan, the merge-path kernels of crs.cu with the structure's thread
+//     coordinates as tile boundaries (one CTA per VNEC thread) when a thread
+//     holds at most one tile of items, else a fresh merge-path split;
 //   D (:282-446): one CTA per VNEC thread; its compacted x (use_x_indices)
 //     is staged in shared memory, each row's nLanes-wide column groups are
 //     read as val_align windows (lanes = (group, lane) pairs, coalesced), the
@@ -17,6 +19,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "crs_merge.cuh"
@@ -178,6 +181,12 @@ int vnec_spmv_impl(const rvvla_vnec* A, X alpha, const X* x, X beta, X* y, cudaS
     }
     return RVVLA_OK;
   }
+  // L with the analysed plan: the CRS lane-run kernel on the source arrays
+  if (A->plan && (A->plan_kind == 1 || A->plan_kind == 2)) {
+    const rvvla_crs c{A->m, A->n, A->nz, A->ptr, A->indices, A->val, A->plan, A->plan_tiles, A->plan_kind};
+    if constexpr (std::is_same<X, double>::value) return rvvla_crs_spmv_f64(&c, alpha, x, beta, y, (void*)st);
+    else return rvvla_crs_spmv_f32(&c, alpha, x, beta, y, (void*)st);
+  }
   // L: merge path
   const int64_t tile = (int64_t)kMergeBlock * IPT;
   const int64_t ipt = (A->nz + A->m + NT - 1) / NT;
@@ -265,6 +274,17 @@ int vnec_build_typed(const rvvla_crs* src, int64_t NT, int variant, rvvla_vnec_o
   h.val_align = out->val_align; h.tasks = out->tasks; h.task_start = out->task_start; h.task_end = out->task_end;
   h.spvv_len = out->spvv_len; h.row_begin = out->row_begin; h.row_end = out->row_end;
   h.reorder_col = out->reorder_col; h.reorder_nnz = out->reorder_nnz;
+  if (H.variant == 2 && nz > 0) {
+    // L: analyse the source CRS once for the CRS lane-run kernel
+    const int dt = sizeof(T) == 8 ? RVVLA_F64 : RVVLA_F32;
+    const int64_t plen = rvvla_crs_plan_len(m, nz, dt);
+    RVVLA_CUDA(cudaMalloc(&out->plan, (size_t)std::max<int64_t>(plen, 1) * sizeof(int32_t)));
+    const rvvla_crs c{m, src->n, nz, out->ptr, out->indices, out->val, nullptr, 0, 0};
+    int64_t tiles = 0;
+    int32_t kind = 0;
+    if ((rc = rvvla_crs_analyze(&c, dt, out->plan, &tiles, &kind, st))) return rc;
+    h.plan = out->plan; h.plan_tiles = tiles; h.plan_kind = kind;
+  }
   RVVLA_CUDA(cudaStreamSynchronize(st));
   return RVVLA_OK;
 }
@@ -302,7 +322,7 @@ void rvvla_vnec_free(rvvla_vnec_owned* h) {
   if (!h) return;
   void* ptrs[] = {h->ptr, h->indices, h->val, h->thread_coord_start, h->thread_coord_end, h->ecr_indices, h->NEC_NUM,
                   h->use_x_ptr, h->use_x_indices, h->v_row_ptr, h->col_start, h->val_align, h->tasks, h->task_start,
-                  h->task_end, h->spvv_len, h->row_begin, h->row_end, h->reorder_col, h->reorder_nnz};
+                  h->task_end, h->spvv_len, h->row_begin, h->row_end, h->reorder_col, h->reorder_nnz, h->plan};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   std::memset(h, 0, sizeof(*h));

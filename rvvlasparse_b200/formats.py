@@ -310,7 +310,8 @@ class spMtxVNEC(_GpuFormat):
     """``spMtxVNEC<ValT>`` (include/VNEC.h:35-76).  Unlike the reference (which
     keeps a pointer to the source CRS), the source arrays are copied in."""
 
-    SCALARS = ("m", "n", "nz", "NUM_THREADS_VNEC", "nLanes", "vnec_t", "max_nec", "ngroups", "ntasks", "nreorder")
+    SCALARS = ("m", "n", "nz", "NUM_THREADS_VNEC", "nLanes", "vnec_t", "max_nec", "ngroups", "ntasks", "nreorder",
+               "plan_tiles", "plan_kind")
     ARRAYS = {k: (None if k in ("val", "val_align", "reorder_nnz") else torch.int32) for k in _capi.VNEC_ARRAYS}
     CDESC = _capi.rvvla_vnec
     VALUE = "val"
@@ -341,6 +342,9 @@ def _vnec_convert(dist, src: spMtxCRS, params: convertParams) -> None:
             sizes.update({"NEC_NUM": NT, "use_x_ptr": NT + 1, "tasks": h.ntasks, "task_start": NT, "task_end": NT,
                           "spvv_len": NT, "row_begin": h.ntasks, "row_end": h.ntasks, "reorder_col": h.nreorder,
                           "reorder_nnz": h.nreorder})
+        if owned.plan:  # L variant: the analysed plan of the source CRS
+            sizes["plan"] = lib.rvvla_crs_plan_len(h.m, h.nz, _capi.RVVLA_F64 if src.dtype == torch.float64
+                                                    else _capi.RVVLA_F32)
         if h.vnec_t in (0, 1):
             # use_x_indices length = use_x_ptr[NT]: read it back
             tmp = _owned_to_tensor(owned.use_x_ptr, NT + 1, torch.int32, src.Val.device)

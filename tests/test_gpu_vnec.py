@@ -63,6 +63,13 @@ def test_vnec_structure_and_spmv(g, threads, variant):
     yref = O.crs_spmv_ld(O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"]), g["alpha"], g["x"], g["beta"], g["y0"])
     assert O.normwise_relerr(y, yref) < tol_for(g["Val"].dtype)
     assert O.normwise_relerr(y, O.spmv(o, g["alpha"], g["x"], g["beta"], g["y0"])) < tol_for(g["Val"].dtype)
+    if variant == 2 and len(g["Col"]) > 0:
+        # L runs the CRS lane-run kernel on the analysed plan; without the
+        # plan, the merge path over the VNEC threads' coordinates
+        assert V.plan is not None and V.plan_kind in (1, 2)
+        V.plan, V.plan_kind, V.plan_tiles = None, 0, 0
+        y2 = run(V, g["alpha"], g["x"], g["beta"], g["y0"])
+        assert O.normwise_relerr(y2, yref) < tol_for(g["Val"].dtype)
 
 
 def test_vnec_variant_rule_and_ird():
