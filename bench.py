@@ -485,9 +485,9 @@ def form_batched(torch, pk):
 
 def form_adjoint(torch, pk):
     """y = A(v) x on a random matrix (n = 1,048,576, geometric rows of mean
-    19, uniform columns, fp32 N(0,1) values): forward, dx = A^T g (values
-    refreshed through the permutation, CRS kernels on the GPU-built
-    transpose) and dvalues = g_i x_j (SDDMM); the transpose build is timed
+    19, uniform columns, fp32 N(0,1) values): forward, dx = A^T g (the CRS
+    lane-run kernel on the GPU-built transpose, A's values read through the
+    permutation) and dvalues = g_i x_j (SDDMM); the transpose build is timed
     once."""
     import time as _t
 
@@ -507,9 +507,10 @@ def form_adjoint(torch, pk):
     x = torch.randn(n, device="cuda")
     g = torch.randn(m, device="cuda")
     fwd = 8 * nnz + 4 * (m + 1) + 4 * n + 4 * m
+    adj = 12 * nnz + 4 * (n + 1) + 4 * m + 4 * n  # A^T columns, permutation, values through it
     sdd = 8 * nnz + 4 * (m + 1) + 4 * m + 4 * n
     out = {"workload": f"random rows n={m} nnz={nnz} fp32", "transpose_build_ms": round(build_ms, 2)}
-    for name, fn, b in (("forward", lambda: P.forward(v, x, 1.0), fwd), ("dx", lambda: P.adjoint_x(v, g, 1.0), fwd),
+    for name, fn, b in (("forward", lambda: P.forward(v, x, 1.0), fwd), ("dx", lambda: P.adjoint_x(v, g, 1.0), adj),
                         ("dvalues", lambda: P.sddmm(g, x), sdd)):
         ms = _time_ms(torch, fn)
         out[name] = {"ms": round(ms, 4), "gbs": round(b / (ms * 1e-3) / 1e9, 1),

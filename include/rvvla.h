@@ -106,8 +106,9 @@ typedef struct rvvla_crs {
 /* Size in int32 entries of the plan buffer for rvvla_crs_analyze (the tile
  * size depends on the value type: RVVLA_F64 or RVVLA_F32; mixed uses F32). */
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype);
-/* Analyses the row structure once (synchronises `stream`) for the warp-
- * stream kernel (2048 nonzeros per warp): matrices without empty rows get
+/* Analyses the row structure once (synchronises `stream`) for the lane-run
+ * kernel (256 to 2048 nonzeros per warp by matrix size, 8 per lane, plus a
+ * row-start bitmap of one bit per nonzero): matrices without empty rows get
  * kind 1 (first row of each warp range; plan_tiles = warps), matrices with
  * empty rows kind 2 (the non-empty rows compacted with a map back to their
  * ids and the list of empty rows; plan_tiles = non-empty rows), matrices
@@ -522,6 +523,13 @@ int rvvla_spmv_adjoint_x_f64(const rvvla_transpose* T, double alpha, const doubl
                              double beta, double* dx, void* stream);
 int rvvla_spmv_adjoint_x_f32(const rvvla_transpose* T, float alpha, const float* g,
                              float beta, float* dx, void* stream);
+/* The same product with A's current values Val (nz entries, A's order) read
+ * through the transpose's permutation inside the kernel: no
+ * rvvla_csr_transpose_values pass, A^T's own value array is not used. */
+int rvvla_spmv_adjoint_x_values_f64(const rvvla_transpose* T, const double* Val, double alpha,
+                                    const double* g, double beta, double* dx, void* stream);
+int rvvla_spmv_adjoint_x_values_f32(const rvvla_transpose* T, const float* Val, float alpha,
+                                    const float* g, float beta, float* dx, void* stream);
 /* dvalues[k] = g[row(k)] * x[Col[k]] for every nonzero k of A. */
 int rvvla_sddmm_values_f64(const rvvla_crs* A, const double* g, const double* x, double* dvalues,
                            void* stream);

@@ -235,6 +235,8 @@ def load():
     _proto(lib, "rvvla_csr_transpose_values", cint, P(rvvla_transpose), vp, vp, vp)
     _proto(lib, "rvvla_spmv_adjoint_x_f64", cint, P(rvvla_transpose), dbl, vp, dbl, vp, vp)
     _proto(lib, "rvvla_spmv_adjoint_x_f32", cint, P(rvvla_transpose), flt, vp, flt, vp, vp)
+    _proto(lib, "rvvla_spmv_adjoint_x_values_f64", cint, P(rvvla_transpose), vp, dbl, vp, dbl, vp, vp)
+    _proto(lib, "rvvla_spmv_adjoint_x_values_f32", cint, P(rvvla_transpose), vp, flt, vp, flt, vp, vp)
     _proto(lib, "rvvla_sddmm_values_f64", cint, P(rvvla_crs), vp, vp, vp, vp)
     _proto(lib, "rvvla_sddmm_values_f32", cint, P(rvvla_crs), vp, vp, vp, vp)
     # batched

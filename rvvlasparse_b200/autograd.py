@@ -4,10 +4,11 @@
 CRS sparsity pattern fixed in a :class:`CrsPattern`; its backward runs the
 library's adjoint kernels through the C ABI:
 
-* dx = alpha * A^T g — ``rvvla_spmv_adjoint_x_*`` on the transposed CRS built
-  once per pattern by ``rvvla_csr_transpose``; A^T's values are refreshed
-  from the current ``values`` through the stored permutation
-  (``rvvla_csr_transpose_values``) before each product;
+* dx = alpha * A^T g — ``rvvla_spmv_adjoint_x_values_*`` on the transposed
+  CRS built once per pattern by ``rvvla_csr_transpose``, reading the current
+  ``values`` through the stored permutation inside the kernel
+  (``adjoint_x_refreshed`` goes through ``rvvla_csr_transpose_values`` and
+  ``rvvla_spmv_adjoint_x_*`` instead);
 * dvalues[k] = alpha * g[row(k)] * x[Col[k]] — ``rvvla_sddmm_values_*``.
 
 The reference has no adjoint (it declares SPARSE_OPERATION_TRANSPOSE in
@@ -73,6 +74,19 @@ class CrsPattern:
         return y
 
     def adjoint_x(self, values: torch.Tensor, g: torch.Tensor, alpha: float) -> torch.Tensor:
+        """dx = alpha * A(values)^T g; the values are read through the
+        transpose's permutation inside the kernel."""
+        lib = load()
+        dx = torch.empty(self.n, dtype=self.dtype, device=g.device)
+        fn = (lib.rvvla_spmv_adjoint_x_values_f64 if self.dtype == torch.float64
+              else lib.rvvla_spmv_adjoint_x_values_f32)
+        check(fn(C.byref(self._tr.h), _ptr(values), float(alpha), _ptr(g), 0.0, _ptr(dx), _stream()),
+              "spmv_adjoint_x_values")
+        return dx
+
+    def adjoint_x_refreshed(self, values: torch.Tensor, g: torch.Tensor, alpha: float) -> torch.Tensor:
+        """The same product through rvvla_csr_transpose_values (A^T's own
+        value array re-gathered first) and rvvla_spmv_adjoint_x."""
         lib = load()
         check(lib.rvvla_csr_transpose_values(C.byref(self._tr.h), _ptr(values), self._tr.Val, _stream()),
               "csr_transpose_values")

@@ -67,62 +67,46 @@ __global__ void tr_gather_kernel(int64_t nz, const int* __restrict__ perm, const
   if (val) static_cast<W*>(ValT)[k] = static_cast<const W*>(val)[p];
 }
 
-// largest r in [lo, hi] with Rst[r] <= k (the row holding nonzero k)
-__device__ __forceinline__ int64_t row_search(const int* __restrict__ Rst, int64_t lo, int64_t hi, int64_t k) {
-  while (lo < hi) {
-    const int64_t mid = (lo + hi + 1) >> 1;
-    if ((int64_t)Rst[mid] <= k) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 constexpr int kSdThreads = 256;
-constexpr int kSdItems = 8;
-constexpr int kSdBlock = kSdThreads * kSdItems;  // nonzeros per CTA
-constexpr int kSdWindow = 4096;                  // row pointers staged in shared memory
+constexpr int kSdRows = 256;  // rows per CTA
+constexpr int kSdU = 4;       // nonzeros per thread in flight
 
-// dv[k] = g[row(k)] * x[Col[k]]: a CTA per 2048 consecutive nonzeros, the row
-// pointers covering them staged in shared memory (matrices with many empty
-// rows in one range search the global row pointer instead).
+// dv[k] = g[row(k)] * x[Col[k]]: a CTA per 256 consecutive rows, their row
+// pointers staged in shared memory (no search in global memory); each thread
+// takes every 256th nonzero of the CTA's range, finds its row by binary
+// search over the staged pointers and keeps 4 nonzeros' loads in flight.
 template <class T>
 __global__ void __launch_bounds__(kSdThreads)
-sddmm_kernel(int64_t m, int64_t nz, const int* __restrict__ Rst, const int* __restrict__ Col,
-             const T* __restrict__ g, const T* __restrict__ x, T* __restrict__ dv) {
-  __shared__ int win[kSdWindow];
-  __shared__ int64_t s_r0, s_r1;
-  const int64_t k0 = (int64_t)blockIdx.x * kSdBlock;
-  const int64_t k1 = min(nz, k0 + (int64_t)kSdBlock);
-  if (threadIdx.x == 0) {
-    s_r0 = row_search(Rst, 0, m - 1, k0);
-    s_r1 = row_search(Rst, s_r0, m - 1, k1 - 1);
-  }
+sddmm_kernel(int64_t m, const int* __restrict__ Rst, const int* __restrict__ Col, const T* __restrict__ g,
+             const T* __restrict__ x, T* __restrict__ dv) {
+  __shared__ int win[kSdRows + 1];
+  const int64_t r0 = (int64_t)blockIdx.x * kSdRows;
+  const int nr = (int)min((int64_t)kSdRows, m - r0);
+  for (int i = threadIdx.x; i <= nr; i += kSdThreads) win[i] = Rst[r0 + i];
   __syncthreads();
-  const int64_t r0 = s_r0, r1 = s_r1;
-  const int64_t nw = r1 - r0 + 1;  // candidate rows
-  const bool staged = nw <= kSdWindow;
-  if (staged)
-    for (int64_t i = threadIdx.x; i < nw; i += kSdThreads) win[i] = Rst[r0 + i];
-  __syncthreads();
+  const int kb = win[0], ke = win[nr];
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+  for (int k0 = kb + (int)threadIdx.x; k0 < ke; k0 += kSdU * kSdThreads) {
+    int c[kSdU];
+    T gv[kSdU];
 #pragma unroll
-  for (int it = 0; it < kSdItems; ++it) {
-    const int64_t k = k0 + (int64_t)it * kSdThreads + threadIdx.x;
-    if (k >= k1) break;
-    int64_t r;
-    if (staged) {
-      int64_t lo = 0, hi = nw - 1;
+    for (int u = 0; u < kSdU; ++u) {
+      const int k = min(k0 + u * kSdThreads, ke - 1);
+      int lo = 0, hi = nr - 1;  // largest j with win[j] <= k
       while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if ((int64_t)win[mid] <= k) lo = mid;
+        const int mid = (lo + hi + 1) >> 1;
+        if (win[mid] <= k) lo = mid;
         else hi = mid - 1;
       }
-      r = r0 + lo;
-    } else {
-      r = row_search(Rst, r0, r1, k);
+      c[u] = ld_stream(Col + k, pf);
+      gv[u] = g[r0 + lo];
     }
-    const int c = ld_stream(Col + k, pf);
-    dv[k] = g[r] * ld_keep(x + c, pl);
+#pragma unroll
+    for (int u = 0; u < kSdU; ++u) {
+      const int k = k0 + u * kSdThreads;
+      const T xv = ld_keep(x + c[u], pl);
+      if (k < ke) dv[k] = gv[u] * xv;
+    }
   }
 }
 
@@ -204,8 +188,8 @@ int sddmm_impl(const rvvla_crs* A, const T* g, const T* x, T* dv, cudaStream_t s
   if (A->m < 0 || A->n < 0 || A->nz < 0) return fail(RVVLA_ERR_INVALID_ARG, "sddmm: bad sizes");
   if (A->nz == 0) return RVVLA_OK;
   if (!A->Rst || !A->Col || !g || !x || !dv) return fail(RVVLA_ERR_INVALID_ARG, "sddmm: null array");
-  const int64_t blocks = (A->nz + kSdBlock - 1) / kSdBlock;
-  sddmm_kernel<T><<<(unsigned)blocks, kSdThreads, 0, st>>>(A->m, A->nz, A->Rst, A->Col, g, x, dv);
+  const int64_t blocks = (A->m + kSdRows - 1) / kSdRows;
+  sddmm_kernel<T><<<(unsigned)blocks, kSdThreads, 0, st>>>(A->m, A->Rst, A->Col, g, x, dv);
   RVVLA_LAUNCHED("sddmm_kernel");
   return RVVLA_OK;
 }

@@ -42,7 +42,16 @@
 
 namespace rvvla {
 
-constexpr int kStreamE = 2048;  // nonzeros per warp in the stream kernel
+// Nonzeros per warp in the stream and lane-run kernels: 2048, halved (down
+// to 256) while the matrix would give fewer than ~6 waves of 4736 warps (148
+// SMs x 32 resident warps), so a medium-size matrix does not leave a large
+// partial last wave.  A function of nz alone: the analysis and the SpMV
+// agree on it.
+int crs_warp_span(int64_t nz) {
+  int E = 2048;
+  while (E > 256 && nz < (int64_t)6 * 4736 * E) E >>= 1;
+  return E;
+}
 
 __global__ void crs_stream_plan_kernel(int m, int nnz, const int* __restrict__ Rst, int E, int nwarps,
                                        int* __restrict__ wrow, int* __restrict__ any_empty) {
@@ -140,15 +149,21 @@ int crs_plan_launch(int64_t m, int64_t nz, const int32_t* Rst, int ipt, int32_t*
   return RVVLA_OK;
 }
 
+// perm/pval (the adjoint): value k of A is pval[perm[k]]; needs an analysed
+// plan (kinds 1 and 2) when A has nonzeros.
 template <class V, class X, class Ac, class P, class CT, int IPT>
-int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStream_t st) {
+int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStream_t st,
+                  const int32_t* perm = nullptr, const V* pval = nullptr) {
   int rc = crs_validate(A, x, y);
   if (rc) return rc;
   if (A->m == 0) return RVVLA_OK;
+  if (perm && A->nz > 0 && !(A->plan && (A->plan_kind == 1 || A->plan_kind == 2)))
+    return fail(RVVLA_ERR_INVALID_ARG, "crs: values through a permutation need an analysed plan");
   if (A->plan && (A->plan_kind == 1 || A->plan_kind == 2)) {  // shared-memory-free stream kernel
     // kind 1: plan_tiles = warps, all rows; kind 2: plan_tiles = number of
     // non-empty rows, the warps run over the compacted rows
-    const int64_t nw = (A->nz + kStreamE - 1) / kStreamE;
+    const int E = crs_warp_span(A->nz);
+    const int64_t nw = (A->nz + E - 1) / E;
     if (A->nz == 0 || (A->plan_kind == 1 && A->plan_tiles != nw) ||
         (A->plan_kind == 2 && (A->plan_tiles <= 0 || A->plan_tiles > A->m)))
       return fail(RVVLA_ERR_INVALID_ARG, "crs: stream plan was built for a different matrix");
@@ -176,19 +191,30 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
     int32_t* crow = sc.as<int32_t>();
     CT* cval = (CT*)(sc.as<char>() + row_bytes);
     const unsigned blocks = (unsigned)((nw * 32 + 255) / 256);
-    if (crs_use_stream_kernel()) {
-      crs_stream_kernel<V, X, Ac, CT><<<blocks, 256, 0, st>>>(mr, (int)A->nz, kStreamE, (int)nw, rst, A->Col,
+    if (perm) {
+      const bool vec = (uintptr_t)A->Col % 16 == 0 && (uintptr_t)perm % 16 == 0;
+      if (vec)
+        crs_run_kernel<V, X, Ac, CT, true, true><<<blocks, 256, 0, st>>>(
+            mr, (int)A->nz, E, (int)nw, rst, bits, A->Col, pval, x, y, alpha, beta, wrow, crow, cval, row_map,
+            perm);
+      else
+        crs_run_kernel<V, X, Ac, CT, false, true><<<blocks, 256, 0, st>>>(
+            mr, (int)A->nz, E, (int)nw, rst, bits, A->Col, pval, x, y, alpha, beta, wrow, crow, cval, row_map,
+            perm);
+      RVVLA_LAUNCHED("crs_run_kernel");
+    } else if (crs_use_stream_kernel()) {
+      crs_stream_kernel<V, X, Ac, CT><<<blocks, 256, 0, st>>>(mr, (int)A->nz, E, (int)nw, rst, A->Col,
                                                               (const V*)A->Val, x, y, alpha, beta, wrow, crow, cval,
                                                               row_map);
       RVVLA_LAUNCHED("crs_stream_kernel");
     } else {
       const bool vec = (uintptr_t)A->Col % 16 == 0 && (uintptr_t)A->Val % 16 == 0;
       if (vec)
-        crs_run_kernel<V, X, Ac, CT, true><<<blocks, 256, 0, st>>>(mr, (int)A->nz, kStreamE, (int)nw, rst, bits,
+        crs_run_kernel<V, X, Ac, CT, true><<<blocks, 256, 0, st>>>(mr, (int)A->nz, E, (int)nw, rst, bits,
                                                                    A->Col, (const V*)A->Val, x, y, alpha, beta, wrow,
                                                                    crow, cval, row_map);
       else
-        crs_run_kernel<V, X, Ac, CT, false><<<blocks, 256, 0, st>>>(mr, (int)A->nz, kStreamE, (int)nw, rst, bits,
+        crs_run_kernel<V, X, Ac, CT, false><<<blocks, 256, 0, st>>>(mr, (int)A->nz, E, (int)nw, rst, bits,
                                                                     A->Col, (const V*)A->Val, x, y, alpha, beta, wrow,
                                                                     crow, cval, row_map);
       RVVLA_LAUNCHED("crs_run_kernel");
@@ -232,7 +258,7 @@ extern "C" {
 
 int64_t rvvla_crs_plan_len(int64_t m, int64_t nz, int dtype) {
   const int ipt = dtype == RVVLA_F64 ? MergeCfg<double>::IPT : MergeCfg<float>::IPT;
-  const int64_t nw = (nz + kStreamE - 1) / kStreamE;
+  const int64_t nw = (nz + 255) / 256;  // the most warps any span gives
   return std::max<int64_t>(2 * (crs_tiles(m, nz, ipt) + 1), 3 * m + nw + 3 + (nz + 31) / 32);
 }
 
@@ -247,12 +273,13 @@ int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* pla
   if (A->m == 0) return RVVLA_OK;
   cudaStream_t st = as_stream(stream);
   if (A->nz > 0) {
-    const int64_t nw = (A->nz + kStreamE - 1) / kStreamE;
+    const int E = crs_warp_span(A->nz);
+    const int64_t nw = (A->nz + E - 1) / E;
     Scratch flag;
     RVVLA_CUDA(flag.alloc(sizeof(int), st));
     RVVLA_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
     const int64_t n = std::max<int64_t>(nw, A->m);
-    crs_stream_plan_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((int)A->m, (int)A->nz, A->Rst, kStreamE,
+    crs_stream_plan_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((int)A->m, (int)A->nz, A->Rst, E,
                                                                          (int)nw, plan, flag.as<int>());
     RVVLA_LAUNCHED("crs_stream_plan_kernel");
     int any_empty = 1;
@@ -287,7 +314,7 @@ int rvvla_crs_analyze(const rvvla_crs* A, int dtype, int32_t* plan, int64_t* pla
     int32_t* empty = row_map + mc;
     crs_compact_kernel<<<mb, 256, 0, st>>>((int)A->m, (int)A->nz, A->Rst, s_pos.as<int64_t>(), rst_c, row_map, empty);
     RVVLA_LAUNCHED("crs_compact_kernel");
-    crs_stream_plan_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>((int)mc, (int)A->nz, rst_c, kStreamE,
+    crs_stream_plan_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>((int)mc, (int)A->nz, rst_c, E,
                                                                          (int)nw, wrow, flag.as<int>());
     RVVLA_LAUNCHED("crs_stream_plan_kernel");
     uint32_t* bits = reinterpret_cast<uint32_t*>(empty + me);
@@ -316,6 +343,22 @@ int rvvla_crs_spmv_f64(const rvvla_crs* A, double alpha, const double* x, double
 int rvvla_crs_spmv_f32(const rvvla_crs* A, float alpha, const float* x, float beta, float* y, void* stream) {
   return crs_spmv_impl<float, float, float, float, float, MergeCfg<float>::IPT>(A, alpha, x, beta, y,
                                                                                as_stream(stream));
+}
+
+int rvvla_spmv_adjoint_x_values_f64(const rvvla_transpose* T, const double* Val, double alpha, const double* g,
+                                    double beta, double* dx, void* stream) {
+  if (!T || T->val_bytes != 8) return fail(RVVLA_ERR_INVALID_ARG, "spmv_adjoint_x_values_f64: needs an fp64 transpose");
+  if (T->AT.nz > 0 && (!T->perm || !Val)) return fail(RVVLA_ERR_INVALID_ARG, "spmv_adjoint_x_values_f64: null array");
+  return crs_spmv_impl<double, double, double, double, double, MergeCfg<double>::IPT>(&T->AT, alpha, g, beta, dx,
+                                                                                      as_stream(stream), T->perm, Val);
+}
+
+int rvvla_spmv_adjoint_x_values_f32(const rvvla_transpose* T, const float* Val, float alpha, const float* g,
+                                    float beta, float* dx, void* stream) {
+  if (!T || T->val_bytes != 4) return fail(RVVLA_ERR_INVALID_ARG, "spmv_adjoint_x_values_f32: needs an fp32 transpose");
+  if (T->AT.nz > 0 && (!T->perm || !Val)) return fail(RVVLA_ERR_INVALID_ARG, "spmv_adjoint_x_values_f32: null array");
+  return crs_spmv_impl<float, float, float, float, float, MergeCfg<float>::IPT>(&T->AT, alpha, g, beta, dx,
+                                                                               as_stream(stream), T->perm, Val);
 }
 
 int rvvla_crs_spmv_mixed(const rvvla_crs* A, int val_type, float alpha, const float* x, float beta, float* y,

@@ -71,13 +71,15 @@ template <> struct RunVec<__nv_bfloat16> {
 
 // rst: row starts of the rows the warps walk (all rows, or the compacted
 // non-empty rows with row_map back to the ids); bits: the row-start bitmap
-// over the nonzeros; VEC: Col and Val are 16-byte aligned (vector loads).
-template <class V, class X, class Ac, class CT, bool VEC>
+// over the nonzeros; VEC: Col and Val (or perm) are 16-byte aligned (vector
+// loads); PERM: value k is Val[perm[k]] (the adjoint reads A's values
+// through the transpose's permutation instead of a re-gathered copy).
+template <class V, class X, class Ac, class CT, bool VEC, bool PERM = false>
 __global__ void __launch_bounds__(256)
 crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, const uint32_t* __restrict__ bits,
                const int* __restrict__ Col, const V* __restrict__ Val, const X* __restrict__ x, X* __restrict__ y,
                X alpha, X beta, const int* __restrict__ wrow, int* __restrict__ carry_row, CT* __restrict__ carry_val,
-               const int* __restrict__ row_map) {
+               const int* __restrict__ row_map, const int* __restrict__ perm = nullptr) {
   const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (w >= nwarps) return;
@@ -111,13 +113,22 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
       const int4 c23 = ld_v4_l1(Col + a + 4, pf);
       cidx[0] = c01.x; cidx[1] = c01.y; cidx[2] = c01.z; cidx[3] = c01.w;
       cidx[4] = c23.x; cidx[5] = c23.y; cidx[6] = c23.z; cidx[7] = c23.w;
-      RunVec<V>::load(Val + a, vv, pf);
+      if constexpr (PERM) {
+        const int4 p01 = ld_v4_l1(perm + a, pf);
+        const int4 p23 = ld_v4_l1(perm + a + 4, pf);
+        const int pi[kRunLane] = {p01.x, p01.y, p01.z, p01.w, p23.x, p23.y, p23.z, p23.w};
+#pragma unroll
+        for (int i = 0; i < kRunLane; ++i) vv[i] = Val[pi[i]];
+      } else {
+        RunVec<V>::load(Val + a, vv, pf);
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < kRunLane; ++i) {
         const int k = i < nv ? a + i : kb;  // idle slots read a valid nonzero
         cidx[i] = ld_stream(Col + k, pf);
-        vv[i] = ld_stream(Val + k, pf);
+        if constexpr (PERM) vv[i] = Val[ld_stream(perm + k, pf)];
+        else vv[i] = ld_stream(Val + k, pf);
       }
     }
     using PT = decltype(vmul(V(), X()));

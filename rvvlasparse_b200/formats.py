@@ -668,12 +668,11 @@ def _call_transpose(mat: "spMtxCRS", alpha, b, beta, y) -> int:
             return st
         tr = (_TransposeHandle(owned), key)
         mat._transpose = tr
-    else:  # same pattern: refresh the values (they may have changed in place)
-        st = lib.rvvla_csr_transpose_values(C.byref(tr[0].owned.h), _ptr(mat.Val), tr[0].owned.Val, _stream())
-        if st != 0:
-            return st
-    fn = lib.rvvla_spmv_adjoint_x_f64 if mat.dtype == torch.float64 else lib.rvvla_spmv_adjoint_x_f32
-    return fn(C.byref(tr[0].owned.h), float(alpha), _ptr(b), float(beta), _ptr(y), _stream())
+    # the current values (they may have changed in place) are read through
+    # the transpose's permutation
+    fn = (lib.rvvla_spmv_adjoint_x_values_f64 if mat.dtype == torch.float64
+          else lib.rvvla_spmv_adjoint_x_values_f32)
+    return fn(C.byref(tr[0].owned.h), _ptr(mat.Val), float(alpha), _ptr(b), float(beta), _ptr(y), _stream())
 
 
 class _TransposeHandle:

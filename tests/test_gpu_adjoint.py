@@ -35,7 +35,7 @@ def test_transpose_bit_exact(g):
     P = pattern(g["m"], g["n"], g["Rst"], g["Col"], dt)
     vals = dev(g["Val"])
     gvec = dev(g["y0"])
-    P.adjoint_x(vals, gvec, 1.0)  # refreshes A^T's values
+    P.adjoint_x_refreshed(vals, gvec, 1.0)  # refreshes A^T's values
     torch.cuda.synchronize()
     t = {k: v.cpu().numpy() for k, v in P.transposed().items()}
     o = O.transpose(O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"]))
@@ -54,6 +54,9 @@ def test_adjoint_x_and_sddmm(g):
     At = O.transpose(A)
     ref = O.crs_spmv_ld(At, 1.5, gv, 0.0, np.zeros(n))
     assert O.normwise_relerr(dx, ref) < tol_for(dt)
+    # through the re-gathered A^T values: the same sums in the same order
+    dx2 = P.adjoint_x_refreshed(vals, dev(gv), 1.5).cpu().numpy()
+    assert np.array_equal(dx, dx2)
     if O.ref_available():  # the reference's own CRS kernel on A^T
         y = O.ref_crs(At).spmv(1.5, gv, 0.0, np.zeros(n, dt))
         assert O.normwise_relerr(dx, y) < tol_for(dt)

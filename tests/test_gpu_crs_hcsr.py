@@ -290,3 +290,35 @@ def test_crs_stream_over_nonempty_rows(empty_frac):
     y0n = np.full(m, np.nan)
     yz = run(A, 1.0, x, 0.0, y0n)
     assert np.all(np.isfinite(yz))
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_crs_run_kernel_unaligned_and_tails(dt):
+    """The lane-run kernel with Col/Val not 16-byte aligned (scalar loads),
+    a nonzero count that leaves a partial chunk and a partial lane, rows of
+    length 1 (8 row starts in a lane), rows ending exactly at lane, chunk and
+    warp boundaries, and a row longer than a warp's span."""
+    rng = np.random.default_rng(5)
+    m, n = 6001, 9000
+    lens = rng.integers(1, 20, m)
+    lens[10:300] = 1
+    lens[400:410] = 8
+    lens[500:508] = 256
+    lens[3000] = 7777
+    Rst = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    nz = int(Rst[-1])
+    assert nz % 8 != 0
+    Col = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    Val = rng.uniform(-1, 1, nz).astype(dt)
+    x, y0 = rng.uniform(-1, 1, n).astype(dt), rng.uniform(-1, 1, m).astype(dt)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 0.5, x, -1.5, y0)
+    tdt = torch.float64 if dt == np.float64 else torch.float32
+    cbig = torch.zeros(nz + 1, dtype=torch.int32, device="cuda")
+    vbig = torch.zeros(nz + 1, dtype=tdt, device="cuda")
+    cbig[1:] = dev(Col)
+    vbig[1:] = dev(Val)
+    for Cv, Vv in ((cbig[1:], vbig[1:]), (dev(Col), dev(Val))):
+        A = R.spMtxCRS(m, n, nz, dev(Rst), Cv, Vv)
+        assert A.plan(0 if dt == np.float64 else 1)[2] == 1
+        y = run(A, 0.5, x, -1.5, y0)
+        assert O.normwise_relerr(y, yref) < tol_for(dt)
