@@ -18,7 +18,10 @@
 //   CSR, k = 1   tpr lanes per row (tpr in {1,2,4,...,32}, per matrix): lanes
 //                stride over the row, shuffle reduction inside the group;
 //   CSR, k > 1   k lanes per row (k in {4, 8, 32}), lane = right-hand side;
-//                the group walks the row, each lane gathers its own X value;
+//                the tile's columns and values (at most 2048 nonzeros) are
+//                staged in shared memory with one coalesced pass, then the
+//                group walks the row from there, each lane gathering its own
+//                X value, 8 nonzeros in flight;
 //   SELL, k = 1  a warp per slice, lane = row, column-major loads;
 //   SELL, k > 1  a warp per slice, lane = row, k accumulators per lane.
 #include <algorithm>
@@ -97,28 +100,52 @@ __device__ void csr_k1(const BatchMat& A, const BatchTile& t, const int* __restr
   }
 }
 
+constexpr int kStageNnz = 2048;  // nonzeros of a k > 1 CSR tile staged in shared memory
+
 template <class T, int K>
-__device__ void csr_kn(const BatchMat& A, const BatchTile& t, const int* __restrict__ srst, const T* __restrict__ X,
-                       T* __restrict__ Y, T alpha, T beta) {
+__device__ void csr_kn(const BatchMat& A, const BatchTile& t, const int* __restrict__ srst, int* __restrict__ s_col,
+                       T* __restrict__ s_val, const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta) {
   constexpr int nslots = kBThreads / K;
+  constexpr int U = 8;
   const int slot = threadIdx.x / K, rhs = threadIdx.x % K;
   const T* __restrict__ x = X + A.x_off + rhs;
   const T* __restrict__ val = static_cast<const T*>(A.Val);
-  const uint64_t pl = policy_evict_last();
-  for (int rr = slot; rr < t.count; rr += nslots) {
-    const int b = srst[rr], e = srst[rr + 1];
-    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
-    int j = b;
-    for (; j + 3 < e; j += 4) {
-      const int c0 = A.Col[j], c1 = A.Col[j + 1], c2 = A.Col[j + 2], c3 = A.Col[j + 3];
-      const T v0 = val[j], v1 = val[j + 1], v2 = val[j + 2], v3 = val[j + 3];
-      s0 += v0 * ld_keep(x + (int64_t)c0 * K, pl);
-      s1 += v1 * ld_keep(x + (int64_t)c1 * K, pl);
-      s2 += v2 * ld_keep(x + (int64_t)c2 * K, pl);
-      s3 += v3 * ld_keep(x + (int64_t)c3 * K, pl);
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+  const int b0 = srst[0], nzt = srst[t.count] - b0;
+  // uniform over the CTA (the tile is shared): stage, or read in place (a
+  // single row longer than the stage)
+  const bool staged = nzt <= kStageNnz;
+  if (staged) {
+    for (int i = threadIdx.x; i < nzt; i += kBThreads) {
+      s_col[i] = ld_stream(A.Col + b0 + i, pf);
+      s_val[i] = ld_stream(val + b0 + i, pf);
     }
-    for (; j < e; ++j) s0 += val[j] * ld_keep(x + (int64_t)A.Col[j] * K, pl);
-    store_y(Y + A.y_off + (int64_t)(t.first + rr) * K + rhs, alpha, beta, (s0 + s1) + (s2 + s3));
+    __syncthreads();
+  }
+  for (int rr = slot; rr < t.count; rr += nslots) {
+    const int b = srst[rr] - b0, e = srst[rr + 1] - b0;
+    T s[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) s[u] = T(0);
+    int j = b;
+    for (; j + U <= e; j += U) {
+      int c[U];
+      T v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        c[u] = staged ? s_col[j + u] : A.Col[b0 + j + u];
+        v[u] = staged ? s_val[j + u] : val[b0 + j + u];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) s[u] += v[u] * ld_keep(x + (int64_t)c[u] * K, pl);
+    }
+    for (; j < e; ++j) {
+      const int c = staged ? s_col[j] : A.Col[b0 + j];
+      const T v = staged ? s_val[j] : val[b0 + j];
+      s[0] += v * ld_keep(x + (int64_t)c * K, pl);
+    }
+    const T r = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+    store_y(Y + A.y_off + (int64_t)(t.first + rr) * K + rhs, alpha, beta, r);
   }
 }
 
@@ -179,6 +206,8 @@ batched_kernel(int64_t ntiles, const BatchTile* __restrict__ tiles, const BatchM
   // metadata (SELL) are copied to shared memory once, then used by all warps
   __shared__ int srst[kTileRowsMax + 1];
   __shared__ int meta[4][kTileSlicesMax];
+  __shared__ int s_col[K > 1 ? kStageNnz : 1];
+  __shared__ T s_val[K > 1 ? kStageNnz : 1];
   __shared__ __align__(16) unsigned char sAraw[sizeof(BatchMat)];
   const BatchMat& A = *reinterpret_cast<const BatchMat*>(sAraw);
   static_assert(sizeof(BatchMat) % 8 == 0, "BatchMat is copied as 8-byte words");
@@ -193,7 +222,7 @@ batched_kernel(int64_t ntiles, const BatchTile* __restrict__ tiles, const BatchM
       for (int i = threadIdx.x; i <= t.count; i += kBThreads) srst[i] = A.Rst[t.first + i];
       __syncthreads();
       if constexpr (K == 1) csr_k1<T>(A, t, srst, X, Y, alpha, beta);
-      else csr_kn<T, K>(A, t, srst, X, Y, alpha, beta);
+      else csr_kn<T, K>(A, t, srst, s_col, s_val, X, Y, alpha, beta);
     } else {
       if (threadIdx.x < t.count) {
         const int sl = t.first + threadIdx.x;
@@ -208,7 +237,7 @@ batched_kernel(int64_t ntiles, const BatchTile* __restrict__ tiles, const BatchM
   }
 }
 
-constexpr int64_t kTileWork = 8192;  // nonzero x right-hand-side products per tile (k = 1: nonzeros)
+constexpr int64_t kTileWork = 8192;  // k = 1 CSR tile: nonzeros + rows; SELL tile: 4x this in products
 
 int default_tpr(double avg) {
   int t = 1;
@@ -351,15 +380,16 @@ int rvvla_batched_plan(const rvvla_crs* mats, int64_t count, int val_bytes, int 
         break;
       }
       b.tpr = (k == 1) ? tpr : k;
-      // tiles of whole rows: at most kTileWork products and at most 8 row
-      // passes of the CTA
-      const int64_t max_rows = std::min<int64_t>((int64_t)(kBThreads / b.tpr) * 8, kTileRowsMax);
+      // tiles of whole rows: k = 1 at most kTileWork nonzeros and 8 row
+      // passes of the CTA; k > 1 at most the staged nonzeros and 32 passes
+      const int64_t max_rows = std::min<int64_t>((int64_t)(kBThreads / b.tpr) * (k == 1 ? 8 : 32), kTileRowsMax);
+      const int64_t max_work = k == 1 ? kTileWork : kStageNnz;
       int64_t r0 = 0;
       while (r0 < A.m) {
         int64_t r1 = r0, work = 0;
         while (r1 < A.m && r1 - r0 < max_rows) {
-          const int64_t wr = ((int64_t)Rst[(size_t)r1 + 1] - Rst[(size_t)r1] + 1) * k;
-          if (r1 > r0 && work + wr > kTileWork) break;
+          const int64_t wr = (int64_t)Rst[(size_t)r1 + 1] - Rst[(size_t)r1] + (k == 1 ? 1 : 0);
+          if (r1 > r0 && work + wr > max_work) break;
           work += wr;
           ++r1;
         }
