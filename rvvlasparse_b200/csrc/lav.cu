@@ -75,32 +75,34 @@ lav_segment_kernel(int64_t s, int64_t L, int64_t cc, const int* __restrict__ co,
 // sparse part has applied beta).  Chunks are cut from rows sorted by dense
 // count, so the long chunks lead and their CTAs start first.
 //
-// Loads: each thread issues all loads of 4 steps before using any (steps
+// Loads: each thread issues all loads of kLavU steps before using any (steps
 // past the chunk's end are clamped to its last step, which holds L slots,
 // and dropped); x is gathered at min(col, n-1) so that padding slots need
 // no mask test first, and a product counts only where the step is active
 // (every lane before fe, the first mask[q] lanes after it).
+constexpr int kLavU = 4;  // steps whose loads are in flight together (8 measured slower)
+
 template <class V, class X, class CT, int L>
 __device__ __forceinline__ CT lav_steps(int q, int qend, int qstride, int fe, int i, int64_t base, int64_t nmax,
                                         const uint16_t* __restrict__ mk, const V* __restrict__ val,
                                         const uint32_t* __restrict__ col, const X* __restrict__ x, uint64_t pf,
                                         uint64_t pl) {
   CT part = 0;
-  for (; q < qend; q += 4 * qstride) {
-    int64_t e[4];
-    uint32_t ci[4];
-    V vv[4];
-    X xv[4];
+  for (; q < qend; q += kLavU * qstride) {
+    int64_t e[kLavU];
+    uint32_t ci[kLavU];
+    V vv[kLavU];
+    X xv[kLavU];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) e[u] = base + min(q + u * qstride, qend - 1);
+    for (int u = 0; u < kLavU; ++u) e[u] = base + min(q + u * qstride, qend - 1);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) ci[u] = ld_stream(col + e[u] * L + i, pf);
+    for (int u = 0; u < kLavU; ++u) ci[u] = ld_stream(col + e[u] * L + i, pf);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) vv[u] = ld_stream(val + e[u] * L + i, pf);
+    for (int u = 0; u < kLavU; ++u) vv[u] = ld_stream(val + e[u] * L + i, pf);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) xv[u] = ld_keep(x + min((int64_t)ci[u], nmax), pl);
+    for (int u = 0; u < kLavU; ++u) xv[u] = ld_keep(x + min((int64_t)ci[u], nmax), pl);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < kLavU; ++u) {
       const int qq = q + u * qstride;
       if (qq < qend && (qq < fe || i < (int)mk[e[u]])) part += (CT)vmul(vv[u], xv[u]);
     }
