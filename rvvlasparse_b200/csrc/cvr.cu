@@ -15,10 +15,11 @@
 //
 // SpMV: y *= beta first (as the reference, :115-117), then one warp per
 // range (lane = CVR lane): coalesced 32-wide vector loads (L2 evict-first),
-// x gathers (evict-last), and per vector the records that fall in it are
-// scattered to their lanes through a 32-entry shared table; a flush is
-// y[row] += alpha * lane_sum.  Each row is flushed by one lane once (zero
-// sums, e.g. idle tail lanes, are skipped), so no atomics are needed.
+// x gathers (evict-last), and per batch of vectors the records that fall in
+// it are scattered to their (vector, lane) slots through a shared table; a
+// flush is y[row] += alpha * lane_sum.  Each row is flushed by one lane once
+// (zero sums, e.g. idle tail lanes, are skipped), so the flush is an atomic
+// add with a single contributor: deterministic.
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -168,7 +169,7 @@ __global__ void cvr_scale_kernel(int64_t m, X* __restrict__ y, X beta) {
   if (i < m) y[i] = (beta == X(0)) ? X(0) : y[i] * beta;
 }
 
-// A warp per CVR thread (lane = SIMD lane), kCvrU vectors per batch.  A
+// A warp per CVR thread (lane = SIMD lane), cvr_batch<V>() vectors per batch.  A
 // batch first issues all loads of its vectors (indices past the range are
 // clamped to its last vector and their products dropped), then marks the
 // records that fall in the batch in a per-warp table (vector in batch, lane)
@@ -178,14 +179,17 @@ __global__ void cvr_scale_kernel(int64_t m, X* __restrict__ y, X beta) {
 // record window_base + l) with the next window prefetched.  A row belongs to
 // one lane of one range, so each row of y receives exactly one contribution:
 // y was scaled by beta first and the flush is a fire-and-forget atomic add
-// (no read of y on the critical path, and still deterministic).
-constexpr int kCvrU = 8;
+// (no read of y on the critical path, and still deterministic).  Vectors per
+// batch: 8 for 8-byte values, 16 for 4-byte ones (about the same bytes in
+// flight).
+template <class V> constexpr int cvr_batch() { return sizeof(V) >= 8 ? 8 : 16; }
 
 template <class V, class X, class CT>
 __global__ void __launch_bounds__(256, 3)
 cvr_spmv_kernel(int64_t NT, int64_t nItems, int64_t nrec, const V* __restrict__ vals,
                 const uint32_t* __restrict__ cols, const int* __restrict__ rec, const int* __restrict__ wb,
                 const X* __restrict__ x, X* __restrict__ y, X alpha) {
+  constexpr int kCvrU = cvr_batch<V>();
   __shared__ int s_row[8][kCvrU][kS];
   const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
