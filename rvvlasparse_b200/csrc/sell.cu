@@ -150,17 +150,19 @@ sell_warp_kernel(int64_t cnt_b, const int* __restrict__ vCl, const int* __restri
         const int64_t base = vCs[s] + lane;
         Ac acc;
         acc_zero(acc);
+        // columns in flight: 4 for 8-byte values, 8 for narrower ones
+        constexpr int U = sizeof(V) >= 8 ? 4 : 8;
         int j = 0;
-        for (; j + 4 <= w; j += 4) {
-          uint32_t c[4];
-          V v[4];
+        for (; j + U <= w; j += U) {
+          uint32_t c[U];
+          V v[U];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+          for (int u = 0; u < U; ++u) {
             c[u] = ld_stream(vCol + base + (int64_t)(j + u) * bs, pf);
             v[u] = ld_stream(vVal + base + (int64_t)(j + u) * bs, pf);
           }
 #pragma unroll
-          for (int u = 0; u < 4; ++u) acc_add(acc, vmul(v[u], ld_keep(x + c[u], pl)));
+          for (int u = 0; u < U; ++u) acc_add(acc, vmul(v[u], ld_keep(x + c[u], pl)));
         }
         for (; j < w; ++j) {
           const uint32_t c = ld_stream(vCol + base + (int64_t)j * bs, pf);
