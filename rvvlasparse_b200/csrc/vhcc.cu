@@ -32,6 +32,7 @@ namespace {
 
 constexpr int kVec = 32;
 constexpr int kMasks = 5;  // log2(32)
+constexpr int kVhccU = 4;  // vectors whose loads are in flight together
 
 // ---------------------------------------------------------------- builder
 __global__ void vhcc_mark_kernel(int64_t m, const int* __restrict__ Rst, uint32_t* __restrict__ endbits,
@@ -159,39 +160,53 @@ vhcc_spmv_kernel(int64_t NT, const int* __restrict__ thr, const uint32_t* __rest
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
   CT res = 0;
   bool pending = false;  // vectors without a row end left partial sums in every lane
-  for (int64_t v = v0; v < v1; ++v) {
-    const int64_t k = v * kVec + lane;
-    const uint32_t c = ld_stream(col + k, pf);
-    const CT prod = (CT)vmul(ld_stream(vals + k, pf), ld_keep(x + c, pl));
-    if ((uint32_t)v != eor) {
-      res += prod;
-      pending = true;
-    } else {
-      // all of those sums belong to the row that opens this vector: fold
-      // them into lane 0 (the reference sums each such vector into its
-      // first slot) before the segmented scan
-      if (pending) {
+  // vectors kVhccU at a time: all their loads are issued first (indices past
+  // the range clamped to its last vector, their products dropped)
+  for (int64_t vb = v0; vb < v1; vb += kVhccU) {
+    uint32_t cc[kVhccU];
+    V av[kVhccU];
+    X xv[kVhccU];
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) res += __shfl_xor_sync(0xffffffffu, res, off);
-        res = (lane == 0) ? res : CT(0);
-        pending = false;
-      }
-      res += prod;
+    for (int u = 0; u < kVhccU; ++u) cc[u] = ld_stream(col + min(vb + u, v1 - 1) * kVec + lane, pf);
 #pragma unroll
-      for (int s = 0; s < kMasks; ++s) {
-        const CT o = __shfl_up_sync(0xffffffffu, res, 1 << s);
-        if ((mk[s] >> lane) & 1u) res += o;
+    for (int u = 0; u < kVhccU; ++u) av[u] = ld_stream(vals + min(vb + u, v1 - 1) * kVec + lane, pf);
+#pragma unroll
+    for (int u = 0; u < kVhccU; ++u) xv[u] = ld_keep(x + cc[u], pl);
+#pragma unroll
+    for (int u = 0; u < kVhccU; ++u) {
+      const int64_t v = vb + u;
+      if (v >= v1) break;
+      const CT prod = (CT)vmul(av[u], xv[u]);
+      if ((uint32_t)v != eor) {
+        res += prod;
+        pending = true;
+      } else {
+        // all of those sums belong to the row that opens this vector: fold
+        // them into lane 0 (the reference sums each such vector into its
+        // first slot) before the segmented scan
+        if (pending) {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) res += __shfl_xor_sync(0xffffffffu, res, off);
+          res = (lane == 0) ? res : CT(0);
+          pending = false;
+        }
+        res += prod;
+#pragma unroll
+        for (int s = 0; s < kMasks; ++s) {
+          const CT o = __shfl_up_sync(0xffffffffu, res, 1 << s);
+          if ((mk[s] >> lane) & 1u) res += o;
+        }
+        const uint32_t wm = mk[kMasks];
+        if ((wm >> lane) & 1u) {
+          const int rank = __popc(wm & ((1u << lane) - 1u));
+          tmp[row_arr[ridx + rank]] = res;
+        }
+        ridx += __popc(wm);
+        const CT carry = ((wm >> 31) & 1u) ? CT(0) : __shfl_sync(0xffffffffu, res, 31);
+        res = (lane == 0) ? carry : CT(0);
+        mk += kMasks + 1;
+        eor = veceor[vidx++];
       }
-      const uint32_t wm = mk[kMasks];
-      if ((wm >> lane) & 1u) {
-        const int rank = __popc(wm & ((1u << lane) - 1u));
-        tmp[row_arr[ridx + rank]] = res;
-      }
-      ridx += __popc(wm);
-      const CT carry = ((wm >> 31) & 1u) ? CT(0) : __shfl_sync(0xffffffffu, res, 31);
-      res = (lane == 0) ? carry : CT(0);
-      mk += kMasks + 1;
-      eor = veceor[vidx++];
     }
   }
 }
