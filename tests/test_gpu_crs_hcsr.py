@@ -225,9 +225,10 @@ def test_host_vectors_end_to_end():
     assert O.normwise_relerr(y, yref) < 1e-12
 
 
-def test_crs_stream_plan_selected_and_edge_rows():
-    # no empty rows -> warp-stream kernel; rows of length 1 (32 heads per
-    # chunk), exactly 32, and one row far longer than a warp range
+def test_crs_all_rows_plan_and_edge_rows():
+    # no empty rows -> lane-run kernel over all rows (plan kind 1); rows of
+    # length 1 (8 row starts per lane), exactly 32, and one row far longer
+    # than a warp range
     rng = np.random.default_rng(1)
     m, n = 9000, 40000
     lens = np.ones(m, np.int64)
@@ -239,7 +240,7 @@ def test_crs_stream_plan_selected_and_edge_rows():
     Col = np.concatenate([np.sort(rng.choice(n, size=int(k), replace=False)) for k in lens]).astype(np.int32)
     Val = rng.uniform(-1, 1, len(Col))
     A = gpu_crs(m, n, Rst, Col, Val)
-    assert A.plan(0)[2] == 1  # stream kind
+    assert A.plan(0)[2] == 1  # all rows
     x, y0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, m)
     yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 0.5, x, 2.0, y0)
     assert O.normwise_relerr(run(A, 0.5, x, 2.0, y0), yref) < 1e-12
@@ -249,8 +250,8 @@ def test_crs_stream_plan_selected_and_edge_rows():
 
 
 def test_crs_plan_kinds_and_merge_path(g):
-    """Matrices with empty rows get the stream kernel over the compacted
-    non-empty rows (kind 2), others the plain stream (kind 1); a descriptor
+    """Matrices with empty rows get the lane-run kernel over the compacted
+    non-empty rows (kind 2), others over all rows (kind 1); a descriptor
     without a plan runs the merge-path kernel.  All agree with the oracle."""
     A = gpu_crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
     has_empty = np.any(np.diff(g["Rst"]) == 0)
@@ -269,7 +270,7 @@ def test_crs_plan_kinds_and_merge_path(g):
 
 
 @pytest.mark.parametrize("empty_frac", [0.05, 0.6, 0.99])
-def test_crs_stream_over_nonempty_rows(empty_frac):
+def test_crs_plan_over_nonempty_rows(empty_frac):
     """Kind 2 with few, many and almost all rows empty, fp64 and fp32, beta
     on the empty rows included; NaN in y must not survive beta = 0."""
     rng = np.random.default_rng(int(empty_frac * 100))
