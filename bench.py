@@ -375,26 +375,18 @@ def _time_ms(torch, fn, warmup=3, iters=20):
 
 
 def form_precision(torch, pk):
-    """27-point stencil on a 128^3 grid (periodic, 56,623,104 nonzeros),
-    values 1 + 0.1 N(0,1), x U[-1,1]: plain fp64 against the mixed forms (fp32
-    or bf16 values, fp32 x/y, compensated fp32 row sums, fp64 carry merges)
-    for CSR5 and HCSR.  Errors are normwise and per-row against the
-    long-double oracle on the fp64 values ("vs_fp64") and on the stored
-    (rounded) values and x ("vs_stored": the accumulation error alone)."""
+    """The 27-point stencil on a 128^3 grid (periodic, 56,623,104 nonzeros,
+    values 1 + 0.1 N(0,1)) and the 4,194,304-row power-law matrix, x U[-1,1]:
+    plain fp64 against the mixed forms (fp32 or bf16 values, fp32 x/y,
+    compensated fp32 row sums, fp64 carry merges) for CSR5 and HCSR, each
+    precision with the parameters the autotuner picks (CSR5 sigma, HCSR block
+    size).  Errors are normwise and per-row against the long-double oracle on
+    the fp64 values ("vs_fp64") and on the stored (rounded) values and x
+    ("vs_stored": the accumulation error alone)."""
     import oracle as O
     import rvvlasparse_b200 as R
+    from rvvlasparse_b200 import autotune as AT
     from rvvlasparse_b200 import workloads as W
-
-    m, n, Rst, Col, Val = W.stencil27(128, seed=3)
-    nnz = len(Col)
-    x = W.vector(n, 0)
-    z = np.zeros(m)
-    A = O.crs(m, n, Rst, Col, Val)
-    ref = O.crs_spmv_ld(A, 1.0, x, 0.0, z)
-    x32 = x.astype(np.float32)
-    ref32 = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val.astype(np.float32)), 1.0, x32.astype(np.float64), 0.0, z)
-    vbf = torch.as_tensor(Val).to(torch.bfloat16).to(torch.float64).numpy()
-    refbf = O.crs_spmv_ld(O.crs(m, n, Rst, Col, vbf), 1.0, x32.astype(np.float64), 0.0, z)
 
     def errs(y, r):
         nz = np.abs(r) > 0
@@ -402,41 +394,58 @@ def form_precision(torch, pk):
         return {"normwise": float(O.normwise_relerr(y, r)), "row_max": float(rel.max()),
                 "row_median": float(np.median(rel))}
 
-    A64 = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
-    A32 = A64.astype(torch.float32)
-    xd64 = torch.as_tensor(x).cuda()
-    xd32 = xd64.float()
-    out = {"workload": f"stencil27 128^3 n={m} nnz={nnz}", "formats": {}}
-    for fmt in ("csr5", "hcsr"):
-        cls, params = (R.spMtxCSR5, dict(omega=32, sigma=16)) if fmt == "csr5" else (R.spMtxHCSR, {})
-        M64, M32 = cls(), cls()
-        R.convert(M64, A64, R.convertParams(**params))
-        R.convert(M32, A32, R.convertParams(**params))
-        Mbf = M32.astype(torch.bfloat16)
-        res = {}
-        for name, M, mixed, xd, vb, xb, rr in (("f64", M64, False, xd64, 8, 8, None), ("mixed_f32", M32, True, xd32, 4, 4, ref32),
-                                                ("mixed_bf16", Mbf, True, xd32, 2, 4, refbf)):
-            y = torch.zeros(m, dtype=xd.dtype, device="cuda")
-            fn = R.sparse_mv_mixed if mixed else R.sparse_mv
+    out = {}
+    for wname, gen in (("stencil27 128^3", lambda: W.stencil27(128, seed=3)),
+                       ("powerlaw", lambda: W.powerlaw(N_DEFAULT, seed=1))):
+        m, n, Rst, Col, Val = gen()
+        nnz = len(Col)
+        x = W.vector(n, 0)
+        z = np.zeros(m)
+        ref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.0, z)
+        x32 = x.astype(np.float32)
+        ref32 = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val.astype(np.float32)), 1.0, x32.astype(np.float64), 0.0, z)
+        vbf = torch.as_tensor(Val).to(torch.bfloat16).to(torch.float64).numpy()
+        refbf = O.crs_spmv_ld(O.crs(m, n, Rst, Col, vbf), 1.0, x32.astype(np.float64), 0.0, z)
+        A64 = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
+        A32 = A64.astype(torch.float32)
+        xd64 = torch.as_tensor(x).cuda()
+        xd32 = xd64.float()
+        wout = {"workload": f"{wname} n={m} nnz={nnz}", "formats": {}}
+        for fmt in ("csr5", "hcsr"):
+            cls = R.spMtxCSR5 if fmt == "csr5" else R.spMtxHCSR
+            res = {}
+            for name, mdt, mixed, xd, vb, xb, rr in (("f64", None, False, xd64, 8, 8, None),
+                                                     ("mixed_f32", torch.float32, True, xd32, 4, 4, ref32),
+                                                     ("mixed_bf16", torch.bfloat16, True, xd32, 2, 4, refbf)):
+                params = AT.tune(fmt, A64, mdt, iters=3)[0]
+                M = cls()
+                R.convert(M, A32 if mixed else A64, R.convertParams(**params))
+                if mdt == torch.bfloat16:
+                    M = M.astype(torch.bfloat16)
+                y = torch.zeros(m, dtype=xd.dtype, device="cuda")
+                fn = R.sparse_mv_mixed if mixed else R.sparse_mv
 
-            def go():
-                st = fn(R.SPARSE_OPERATION_NON_TRANSPOSE, 1.0, M, R.sparse_matrix_descr(), xd, 0.0, y)
-                if st.code:
-                    raise RuntimeError(f"{fmt} {name}: {st.code}")
+                def go():
+                    st = fn(R.SPARSE_OPERATION_NON_TRANSPOSE, 1.0, M, R.sparse_matrix_descr(), xd, 0.0, y)
+                    if st.code:
+                        raise RuntimeError(f"{fmt} {name}: {st.code}")
 
-            ms = _time_ms(torch, go)
-            yh = y.double().cpu().numpy()
-            b = (csr5_bytes(m, n, nnz, M.p, M.omega, M.tile_desc_len, M.num_offsets, vb, xb) if fmt == "csr5"
-                 else hcsr_bytes(M, vb, xb))
-            e = {"ms": round(ms, 4), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
-                 "frac_of_hbm": round(b / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4),
-                 "gnnz_per_s": round(nnz / (ms * 1e-3) / 1e9, 2), "vs_fp64": errs(yh, ref)}
-            if rr is not None:
-                e["vs_stored"] = errs(yh, rr)
-            res[name] = e
-        for name in ("mixed_f32", "mixed_bf16"):
-            res[name]["speedup_vs_f64"] = round(res["f64"]["ms"] / res[name]["ms"], 3)
-        out["formats"][fmt] = res
+                ms = _time_ms(torch, go)
+                yh = y.double().cpu().numpy()
+                b = (csr5_bytes(m, n, nnz, M.p, M.omega, M.tile_desc_len, M.num_offsets, vb, xb) if fmt == "csr5"
+                     else hcsr_bytes(M, vb, xb))
+                e = {"params": params, "ms": round(ms, 4), "gbs": round(b / (ms * 1e-3) / 1e9, 1),
+                     "frac_of_hbm": round(b / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4),
+                     "gnnz_per_s": round(nnz / (ms * 1e-3) / 1e9, 2), "vs_fp64": errs(yh, ref)}
+                if rr is not None:
+                    e["vs_stored"] = errs(yh, rr)
+                res[name] = e
+                del M
+            for name in ("mixed_f32", "mixed_bf16"):
+                res[name]["speedup_vs_f64"] = round(res["f64"]["ms"] / res[name]["ms"], 3)
+            wout["formats"][fmt] = res
+        out[wname] = wout
+        del A64, A32
     return out
 
 
