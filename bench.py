@@ -539,31 +539,58 @@ def run_forms(torch, pk):
 
 
 def e2e_time(cases, args, torch):
-    """Per step: pinned host x -> device, SpMV, device y -> pinned host."""
-    import rvvlasparse_b200 as R
-
+    """Per step and case: pinned host x -> device, SpMV, device y -> pinned
+    host.  Copies in, products and copies out run on three streams, so case
+    i+1's x crosses while case i computes and case i-1's y comes back (a
+    case's device x is refilled only after its product read it, its device y
+    overwritten only after the copy out read it)."""
     stream = torch.cuda.current_stream()
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
     hx = [torch.empty(c.x.numel(), dtype=c.vt, pin_memory=True).copy_(c.x.cpu()) for c in cases]
     hy = [torch.empty(c.y.numel(), dtype=c.vt, pin_memory=True) for c in cases]
     h2d = sum(h.numel() * h.element_size() for h in hx)
     d2h = sum(h.numel() * h.element_size() for h in hy)
+    nc = len(cases)
+    x_free = [None] * nc   # the product of the case's previous step has read x
+    y_free = [None] * nc   # the copy out of the case's previous step has read y
 
     def one():
-        for c, x, y in zip(cases, hx, hy):
-            c.x.copy_(x, non_blocking=True)
+        for i, (c, x, y) in enumerate(zip(cases, hx, hy)):
+            ev_in = torch.cuda.Event()
+            with torch.cuda.stream(s_in):
+                if x_free[i] is not None:
+                    s_in.wait_event(x_free[i])
+                c.x.copy_(x, non_blocking=True)
+                ev_in.record(s_in)
+            stream.wait_event(ev_in)
+            if y_free[i] is not None:
+                stream.wait_event(y_free[i])
             c.launch()
-            y.copy_(c.y, non_blocking=True)
+            ev_prod = torch.cuda.Event()
+            ev_prod.record(stream)
+            x_free[i] = ev_prod
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_prod)
+                y.copy_(c.y, non_blocking=True)
+                ev_out = torch.cuda.Event()
+                ev_out.record(s_out)
+            y_free[i] = ev_out
 
     for _ in range(2):
         one()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    s_in.wait_event(e0)
+    s_out.wait_event(e0)
     for _ in range(args.steps):
         one()
+    for sx in (s_in, s_out):
+        ev = torch.cuda.Event()
+        ev.record(sx)
+        stream.wait_event(ev)
     e1.record(stream)
     torch.cuda.synchronize()
-    _ = R
     return e0.elapsed_time(e1) / args.steps, h2d, d2h
 
 
