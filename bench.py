@@ -240,6 +240,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(v: float, world: int, device: str) -> float:
+    """The slowest rank's value (every rank must call it, in the same order);
+    world 1 returns v unchanged."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gbs(bytes_per_rank: int, world: int, step_ms: float) -> float:
+    """Whole-job throughput of `world` replicas that each move bytes_per_rank
+    in a step whose slowest rank took step_ms."""
+    return bytes_per_rank * world / (step_ms * 1e-3) / 1e9
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -293,20 +312,14 @@ def run_gpu(args):
     for s in range(args.steps):
         for c, (e0, e1) in zip(cases, ev[s]):
             c.kernel_ms.append(e0.elapsed_time(e1))
-    if world > 1:
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
+    step_ms = max_over_ranks(step_ms, world, "cuda")
     total_bytes = sum(c.bytes for c in cases)
-    value = total_bytes * world / (step_ms * 1e-3) / 1e9
+    value = job_gbs(total_bytes, world, step_ms)
 
     # ---- end-to-end through the API with host buffers (H2D x, D2H y inside)
     e2e_ms, h2d, d2h = e2e_time(cases, args, torch)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = total_bytes * world / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = max_over_ranks(e2e_ms, world, "cuda")
+    e2e_value = job_gbs(total_bytes, world, e2e_ms)
 
     pk = peaks()
     per = {}
