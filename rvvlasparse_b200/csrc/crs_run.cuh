@@ -21,7 +21,7 @@
 
 namespace rvvla {
 
-constexpr int kRunLane = 8;                 // nonzeros per lane in a chunk
+constexpr int kRunLane = 8;                 // nonzeros per lane in a chunk (16 measured slower)
 constexpr int kRunChunk = 32 * kRunLane;    // nonzeros per chunk
 
 // 16-byte loads through L1 (a warp's 16-byte pieces are 64 or 32 bytes
@@ -38,7 +38,7 @@ template <class V> struct RunVec;
 template <> struct RunVec<double> {
   __device__ static void load(const double* p, double (&v)[kRunLane], uint64_t pol) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < kRunLane / 2; ++q) {
       const int4 t = ld_v4_l1(p + 2 * q, pol);
       v[2 * q] = __hiloint2double(t.y, t.x);
       v[2 * q + 1] = __hiloint2double(t.w, t.z);
@@ -48,7 +48,7 @@ template <> struct RunVec<double> {
 template <> struct RunVec<float> {
   __device__ static void load(const float* p, float (&v)[kRunLane], uint64_t pol) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kRunLane / 4; ++q) {
       const int4 t = ld_v4_l1(p + 4 * q, pol);
       v[4 * q] = __int_as_float(t.x);
       v[4 * q + 1] = __int_as_float(t.y);
@@ -59,15 +59,30 @@ template <> struct RunVec<float> {
 };
 template <> struct RunVec<__nv_bfloat16> {
   __device__ static void load(const __nv_bfloat16* p, __nv_bfloat16 (&v)[kRunLane], uint64_t pol) {
-    const int4 t = ld_v4_l1(p, pol);
-    const unsigned w[4] = {(unsigned)t.x, (unsigned)t.y, (unsigned)t.z, (unsigned)t.w};
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      v[2 * q] = __ushort_as_bfloat16((unsigned short)(w[q] & 0xFFFFu));
-      v[2 * q + 1] = __ushort_as_bfloat16((unsigned short)(w[q] >> 16));
+    for (int q8 = 0; q8 < kRunLane / 8; ++q8) {
+      const int4 t = ld_v4_l1(p + 8 * q8, pol);
+      const unsigned w[4] = {(unsigned)t.x, (unsigned)t.y, (unsigned)t.z, (unsigned)t.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        v[8 * q8 + 2 * q] = __ushort_as_bfloat16((unsigned short)(w[q] & 0xFFFFu));
+        v[8 * q8 + 2 * q + 1] = __ushort_as_bfloat16((unsigned short)(w[q] >> 16));
+      }
     }
   }
 };
+
+// kRunLane 32-bit indices of a lane with 16-byte loads
+__device__ __forceinline__ void run_idx(const int* p, int (&v)[kRunLane], uint64_t pol) {
+#pragma unroll
+  for (int q = 0; q < kRunLane / 4; ++q) {
+    const int4 t = ld_v4_l1(p + 4 * q, pol);
+    v[4 * q] = t.x;
+    v[4 * q + 1] = t.y;
+    v[4 * q + 2] = t.z;
+    v[4 * q + 3] = t.w;
+  }
+}
 
 // rst: row starts of the rows the warps walk (all rows, or the compacted
 // non-empty rows with row_map back to the ids); bits: the row-start bitmap
@@ -109,14 +124,10 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
     int cidx[kRunLane];
     V vv[kRunLane];
     if (VEC && c0 + kRunChunk <= ke) {
-      const int4 c01 = ld_v4_l1(Col + a, pf);
-      const int4 c23 = ld_v4_l1(Col + a + 4, pf);
-      cidx[0] = c01.x; cidx[1] = c01.y; cidx[2] = c01.z; cidx[3] = c01.w;
-      cidx[4] = c23.x; cidx[5] = c23.y; cidx[6] = c23.z; cidx[7] = c23.w;
+      run_idx(Col + a, cidx, pf);
       if constexpr (PERM) {
-        const int4 p01 = ld_v4_l1(perm + a, pf);
-        const int4 p23 = ld_v4_l1(perm + a + 4, pf);
-        const int pi[kRunLane] = {p01.x, p01.y, p01.z, p01.w, p23.x, p23.y, p23.z, p23.w};
+        int pi[kRunLane];
+        run_idx(perm + a, pi, pf);
 #pragma unroll
         for (int i = 0; i < kRunLane; ++i) vv[i] = Val[pi[i]];
       } else {
