@@ -723,7 +723,9 @@ def run_reference(args):
     value = tot_b / (ms * 1e-3) / 1e9
     cores = O.ref_num_threads()
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": 0,
+        # n_gpus: the N this arm was launched with (its work runs on the host cores)
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "GB/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", str(args.gpus))),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": ",".join(sorted(set(precs))), "data": "synthetic",
         "config": {"workload": f"{args.workload} n={m} nnz={len(Col)}", "cases": [c[0] for c in cases]},
