@@ -49,7 +49,8 @@ typedef enum rvvla_status {
   RVVLA_ERR_UNSUPPORTED = 4,  /* parameter combination not implemented          */
   RVVLA_ERR_TOO_LARGE = 5,    /* size exceeds an index width or a fixed limit   */
   RVVLA_ERR_TIMEOUT = 6,      /* a bounded device-side wait expired             */
-  RVVLA_ERR_NO_DEVICE = 7     /* no CUDA device / not an sm_100 device          */
+  RVVLA_ERR_NO_DEVICE = 7,    /* no CUDA device / not an sm_100 device          */
+  RVVLA_ERR_IO = 8            /* a file could not be opened, read or written    */
 } rvvla_status;
 
 /* element types (for mixed-precision storage) */
@@ -609,6 +610,39 @@ int64_t rvvla_gen_random_rows(int64_t m, int64_t n, int dist, double param, int 
                               uint64_t seed, int32_t* Rst, int32_t* Col, double* Val);
 /* n values U[lo, hi) or N(0,1) (normal != 0). */
 void rvvla_gen_vector(int64_t n, uint64_t seed, int normal, double lo, double hi, double* out);
+
+/* ------------------------------------------------------------ files
+ * Host-side sparse matrices on disk (no device involved).  The reference's
+ * spMtxCRS carries a Matrix Market type code (include/CRS.h:8,17) but ships
+ * no reader, and its test environment names an "mtx to bin" converter
+ * (cmake/TestEnvironment.cmake:62); these provide both. */
+/* A CRS matrix in host memory allocated by the library (malloc);
+ * rvvla_host_crs_free releases the arrays. */
+typedef struct rvvla_host_crs {
+  int64_t m, n, nz;
+  int32_t* Rst;
+  int32_t* Col;
+  double* Val;
+} rvvla_host_crs;
+void rvvla_host_crs_free(rvvla_host_crs* A);
+/* Reads a Matrix Market coordinate file (real / integer / pattern;
+ * general / symmetric / skew-symmetric) into CRS with ascending columns in
+ * every row; duplicate entries are summed in file order.  Errors: RVVLA_ERR_IO
+ * (unreadable), RVVLA_ERR_FORMAT (malformed, index outside the matrix),
+ * RVVLA_ERR_UNSUPPORTED (complex, Hermitian or dense "array" files). */
+int rvvla_mm_read(const char* path, rvvla_host_crs* out);
+/* Writes a CRS matrix as "matrix coordinate real general" (17 digits). */
+int rvvla_mm_write(const char* path, int64_t m, int64_t n, const int32_t* Rst, const int32_t* Col,
+                   const double* Val);
+/* Binary CRS container: 48-byte header ("RVVLACRS", version 1, value bytes,
+ * m, n, nz), then Rst, Col, Val as stored in memory (little-endian). */
+int rvvla_crs_save(const char* path, int64_t m, int64_t n, int64_t nz, const int32_t* Rst,
+                   const int32_t* Col, const void* Val, int val_bytes);
+/* Header of a binary CRS file (checked against the file length). */
+int rvvla_crs_load_info(const char* path, int64_t* m, int64_t* n, int64_t* nz, int* val_bytes);
+/* Arrays of a binary CRS file into caller buffers sized from
+ * rvvla_crs_load_info; the row pointers and columns are validated. */
+int rvvla_crs_load(const char* path, int32_t* Rst, int32_t* Col, void* Val);
 
 #ifdef __cplusplus
 }

@@ -20,6 +20,7 @@ RVVLA_ERR_UNSUPPORTED = 4
 RVVLA_ERR_TOO_LARGE = 5
 RVVLA_ERR_TIMEOUT = 6
 RVVLA_ERR_NO_DEVICE = 7
+RVVLA_ERR_IO = 8
 
 RVVLA_F64 = 0
 RVVLA_F32 = 1
@@ -38,6 +39,10 @@ class RvvlaError(RuntimeError):
     def __init__(self, status: int, where: str, msg: str):
         super().__init__(f"{where}: status {status}: {msg}")
         self.status = status
+
+
+class rvvla_host_crs(C.Structure):
+    _fields_ = [("m", i64), ("n", i64), ("nz", i64), ("Rst", vp), ("Col", vp), ("Val", vp)]
 
 
 class rvvla_crs(C.Structure):
@@ -254,6 +259,13 @@ def load():
     _proto(lib, "rvvla_gen_powerlaw", i64, i64, dbl, dbl, i64, i64, dbl, u64, vp, vp, vp)
     _proto(lib, "rvvla_gen_random_rows", i64, i64, i64, cint, dbl, cint, u64, vp, vp, vp)
     _proto(lib, "rvvla_gen_vector", None, i64, u64, cint, dbl, dbl, vp)
+    cp = C.c_char_p
+    _proto(lib, "rvvla_host_crs_free", None, P(rvvla_host_crs))
+    _proto(lib, "rvvla_mm_read", cint, cp, P(rvvla_host_crs))
+    _proto(lib, "rvvla_mm_write", cint, cp, i64, i64, vp, vp, vp)
+    _proto(lib, "rvvla_crs_save", cint, cp, i64, i64, i64, vp, vp, vp, cint)
+    _proto(lib, "rvvla_crs_load_info", cint, cp, P(i64), P(i64), P(i64), P(cint))
+    _proto(lib, "rvvla_crs_load", cint, cp, vp, vp, vp)
     _lib = lib
     return lib
 

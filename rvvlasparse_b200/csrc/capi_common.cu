@@ -73,6 +73,7 @@ const char* rvvla_status_string(int s) {
     case RVVLA_ERR_TOO_LARGE: return "too large";
     case RVVLA_ERR_TIMEOUT: return "device wait timed out";
     case RVVLA_ERR_NO_DEVICE: return "no CUDA device";
+    case RVVLA_ERR_IO: return "file input/output error";
     default: return "unknown status";
   }
 }

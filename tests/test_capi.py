@@ -23,7 +23,7 @@ def test_library_exports_every_declared_symbol():
 def test_status_strings_and_version():
     lib = _capi.load()
     assert b"sm_100a" in lib.rvvla_version()
-    for s in range(8):
+    for s in range(9):
         assert lib.rvvla_status_string(s)
 
 
