@@ -588,6 +588,23 @@ void rvvla_batched_graph_free(void* graph);
 int rvvla_batched_autotune(const rvvla_crs* mats, int64_t count, int val_bytes, int k, int32_t* mode,
                            int32_t* param, double* tuned_ms, void* stream);
 
+/* ------------------------------------------------------------ solvers
+ * Conjugate gradients for symmetric positive definite A (no reference
+ * counterpart: a caller of the SpMV path).  A is square, has nonzeros and an
+ * rvvla_crs_analyze plan.  x holds the initial guess and receives the
+ * solution; b, x are device vectors.  Each iteration runs q = A p with p.q
+ * fused into the SpMV, then x/r updates with the new r.r fused into the
+ * same pass; no host synchronisation except a read of r.r every
+ * check_every iterations (so up to check_every - 1 iterations may run after
+ * convergence).  Stops when ||r|| <= rtol ||b|| (recurrence residual) or
+ * after max_iter iterations; *iters and *rel_res = ||r|| / ||b|| report
+ * where it stopped (RVVLA_OK either way).  Scratch: 3 vectors of n plus
+ * partials, stream-ordered.  Bitwise reproducible. */
+int rvvla_cg_f64(const rvvla_crs* A, const double* b, double* x, int64_t max_iter, double rtol,
+                 int64_t check_every, int64_t* iters, double* rel_res, void* stream);
+int rvvla_cg_f32(const rvvla_crs* A, const float* b, float* x, int64_t max_iter, double rtol,
+                 int64_t check_every, int64_t* iters, double* rel_res, void* stream);
+
 /* ------------------------------------------------------------ workloads
  * Seeded synthetic matrices on the host (OpenMP), written into caller
  * buffers in two calls: first with NULL arrays to learn nz, then with

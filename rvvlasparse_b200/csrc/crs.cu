@@ -151,14 +151,19 @@ int crs_plan_launch(int64_t m, int64_t nz, const int32_t* Rst, int ipt, int32_t*
 
 // perm/pval (the adjoint): value k of A is pval[perm[k]]; needs an analysed
 // plan (kinds 1 and 2) when A has nonzeros.
+// dot_part (the solvers): the lane-run kernel also writes one partial of
+// x^T (y - beta y) / alpha per warp (see crs_run_kernel), *nparts of them
+// (at most dot_cap); needs an analysed plan.
 template <class V, class X, class Ac, class P, class CT, int IPT>
 int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStream_t st,
-                  const int32_t* perm = nullptr, const V* pval = nullptr) {
+                  const int32_t* perm = nullptr, const V* pval = nullptr, CT* dot_part = nullptr,
+                  int64_t dot_cap = 0, int64_t* nparts = nullptr) {
   int rc = crs_validate(A, x, y);
   if (rc) return rc;
+  if (nparts) *nparts = 0;
   if (A->m == 0) return RVVLA_OK;
-  if (perm && A->nz > 0 && !(A->plan && (A->plan_kind == 1 || A->plan_kind == 2)))
-    return fail(RVVLA_ERR_INVALID_ARG, "crs: values through a permutation need an analysed plan");
+  if ((perm || dot_part) && A->nz > 0 && !(A->plan && (A->plan_kind == 1 || A->plan_kind == 2)))
+    return fail(RVVLA_ERR_INVALID_ARG, "crs: this product needs an analysed plan (rvvla_crs_analyze)");
   if (A->plan && (A->plan_kind == 1 || A->plan_kind == 2)) {  // shared-memory-free stream kernel
     // kind 1: plan_tiles = warps, all rows; kind 2: plan_tiles = number of
     // non-empty rows, the warps run over the compacted rows
@@ -191,7 +196,20 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
     int32_t* crow = sc.as<int32_t>();
     CT* cval = (CT*)(sc.as<char>() + row_bytes);
     const unsigned blocks = (unsigned)((nw * 32 + 255) / 256);
-    if (perm) {
+    if (dot_part) {
+      if (nw > dot_cap) return fail(RVVLA_ERR_TOO_LARGE, "crs: dot partial buffer too small");
+      *nparts = nw;
+      const bool vec = (uintptr_t)A->Col % 16 == 0 && (uintptr_t)A->Val % 16 == 0;
+      if (vec)
+        crs_run_kernel<V, X, Ac, CT, true, false, true><<<blocks, 256, 0, st>>>(
+            mr, (int)A->nz, E, (int)nw, rst, bits, A->Col, (const V*)A->Val, x, y, alpha, beta, wrow, crow, cval,
+            row_map, nullptr, dot_part);
+      else
+        crs_run_kernel<V, X, Ac, CT, false, false, true><<<blocks, 256, 0, st>>>(
+            mr, (int)A->nz, E, (int)nw, rst, bits, A->Col, (const V*)A->Val, x, y, alpha, beta, wrow, crow, cval,
+            row_map, nullptr, dot_part);
+      RVVLA_LAUNCHED("crs_run_kernel");
+    } else if (perm) {
       const bool vec = (uintptr_t)A->Col % 16 == 0 && (uintptr_t)perm % 16 == 0;
       if (vec)
         crs_run_kernel<V, X, Ac, CT, true, true><<<blocks, 256, 0, st>>>(
@@ -248,6 +266,23 @@ int crs_spmv_impl(const rvvla_crs* A, X alpha, const X* x, X beta, X* y, cudaStr
   merge_fixup_kernel<X, CT><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>((int)nt, (int)A->m, crow, cval, y, alpha);
   RVVLA_LAUNCHED("merge_fixup_kernel");
   return RVVLA_OK;
+}
+
+// q = A p with the fused dot (alpha 1, beta 0): part[0..*nparts) sum to
+// p^T A p; used by the solvers.
+int crs_spmv_dot_f64(const rvvla_crs* A, const double* p, double* q, double* part, int64_t cap, int64_t* nparts,
+                     cudaStream_t st) {
+  return crs_spmv_impl<double, double, double, double, double, MergeCfg<double>::IPT>(A, 1.0, p, 0.0, q, st, nullptr,
+                                                                                      nullptr, part, cap, nparts);
+}
+int crs_spmv_dot_f32(const rvvla_crs* A, const float* p, float* q, float* part, int64_t cap, int64_t* nparts,
+                     cudaStream_t st) {
+  return crs_spmv_impl<float, float, float, float, float, MergeCfg<float>::IPT>(A, 1.0f, p, 0.0f, q, st, nullptr,
+                                                                               nullptr, part, cap, nparts);
+}
+int64_t crs_warp_count(int64_t nz) {
+  const int E = crs_warp_span(nz);
+  return (nz + E - 1) / E;
 }
 
 }  // namespace rvvla

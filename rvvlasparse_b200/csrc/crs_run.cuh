@@ -88,13 +88,18 @@ __device__ __forceinline__ void run_idx(const int* p, int (&v)[kRunLane], uint64
 // non-empty rows with row_map back to the ids); bits: the row-start bitmap
 // over the nonzeros; VEC: Col and Val (or perm) are 16-byte aligned (vector
 // loads); PERM: value k is Val[perm[k]] (the adjoint reads A's values
-// through the transpose's permutation instead of a re-gathered copy).
-template <class V, class X, class Ac, class CT, bool VEC, bool PERM = false>
+// through the transpose's permutation instead of a re-gathered copy); DOT:
+// every row piece v that leaves the kernel (stored, or handed on as a carry)
+// also adds x[row] * v to the warp's partial dot_part[w], so the warps'
+// partials sum to x^T (A x) without a second pass over y (the solvers'
+// fused SpMV-dot; square A).
+template <class V, class X, class Ac, class CT, bool VEC, bool PERM = false, bool DOT = false>
 __global__ void __launch_bounds__(256)
 crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, const uint32_t* __restrict__ bits,
                const int* __restrict__ Col, const V* __restrict__ Val, const X* __restrict__ x, X* __restrict__ y,
                X alpha, X beta, const int* __restrict__ wrow, int* __restrict__ carry_row, CT* __restrict__ carry_val,
-               const int* __restrict__ row_map, const int* __restrict__ perm = nullptr) {
+               const int* __restrict__ row_map, const int* __restrict__ perm = nullptr,
+               CT* __restrict__ dot_part = nullptr) {
   const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (w >= nwarps) return;
@@ -108,9 +113,14 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
   int carry0_row = -1;
   CT carry0 = CT(0);
   auto yrow = [&](int r) { return row_map ? row_map[r] : r; };
+  CT dotv = CT(0);  // DOT: this lane's share of x^T (A x)
+  auto dot_add = [&](int r, CT v) {
+    if constexpr (DOT) dotv += (CT)x[yrow(r)] * v;
+  };
   // closes the open row (complete): the warp's first row may have begun in
   // an earlier warp, then it becomes a carry instead of a store
   auto close_open = [&](CT v) {
+    if (lane == 0) dot_add(crow, v);
     if (c_is_first && first_open) {
       carry0_row = crow;
       carry0 = v;
@@ -175,7 +185,10 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
     for (int i = 0; i < kRunLane; ++i) {
       if ((fl >> i) & 1u) {
         if (nf == 0) lead = sum;
-        else write_row(y, yrow(crow + pre + nf), alpha, beta, (X)acc_out(sum));
+        else {
+          write_row(y, yrow(crow + pre + nf), alpha, beta, (X)acc_out(sum));
+          dot_add(crow + pre + nf, (CT)acc_out(sum));
+        }
         ++nf;
         acc_zero(sum);
       }
@@ -206,7 +219,10 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
     // a marked lane's tail closes at the next marked lane; the last one stays open
     const int last = 31 - __clz(marks);
     const CT tailv = (CT)acc_carry(sum) + Tn;
-    if (nf > 0 && lane != last) write_row(y, yrow(crow + pre + nf), alpha, beta, (X)tailv);
+    if (nf > 0 && lane != last) {
+      write_row(y, yrow(crow + pre + nf), alpha, beta, (X)tailv);
+      dot_add(crow + pre + nf, tailv);
+    }
     cval = __shfl_sync(0xffffffffu, tailv, last);
     crow += total;
   }
@@ -215,6 +231,7 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
   if (lane == 0) {
     int c1 = -1;
     CT v1 = CT(0);
+    dot_add(crow, cval);  // the open row's last piece, stored or carried
     if (ends && !(c_is_first && first_open)) {
       write_row(y, yrow(crow), alpha, beta, (X)cval);
     } else if (c_is_first && first_open) {
@@ -228,6 +245,11 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
     carry_val[2 * w] = carry0;
     carry_row[2 * w + 1] = c1;
     carry_val[2 * w + 1] = v1;
+  }
+  if constexpr (DOT) {  // the warp's partial, lanes added in a fixed order
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) dotv += __shfl_xor_sync(0xffffffffu, dotv, d);
+    if (lane == 0) dot_part[w] = dotv;
   }
 }
 

@@ -1,0 +1,96 @@
+"""GPU: conjugate gradients over the CRS path (fused SpMV-dot and fused
+update-dot) against scipy's direct solution and a numpy CG with the same
+recurrences."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+import torch
+
+import rvvlasparse_b200 as R
+from rvvlasparse_b200 import solvers as S
+from rvvlasparse_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def numpy_cg(A, b, rtol, max_iter):
+    x = np.zeros_like(b)
+    r = b - A @ x
+    p = r.copy()
+    rr = r @ r
+    bb = b @ b
+    it = 0
+    while np.sqrt(rr / bb) > rtol and it < max_iter:
+        q = A @ p
+        alpha = rr / (p @ q)
+        x += alpha * p
+        r -= alpha * q
+        rr_new = r @ r
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+        it += 1
+    return x, it
+
+
+def laplace(g, shift=0.0):
+    m, n, Rst, Col, Val = W.laplace2d(g)
+    Val = Val.copy()
+    if shift:
+        for i in range(m):  # diagonal shift keeps A symmetric positive definite
+            k = Rst[i] + np.searchsorted(Col[Rst[i]:Rst[i + 1]], i)
+            Val[k] += shift
+    return m, n, Rst, Col, Val
+
+
+@pytest.mark.parametrize("g,shift", [(40, 0.0), (128, 0.5)])
+def test_cg_fp64_matches_direct_and_numpy_cg(g, shift):
+    m, n, Rst, Col, Val = laplace(g, shift)
+    A = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
+    As = sp.csr_matrix((Val, Col, Rst), shape=(m, n))
+    b = W.vector(n, 7)
+    x, it, rel = S.cg(A, torch.as_tensor(b).cuda(), rtol=1e-10, max_iter=5000, check_every=1)
+    xh = x.cpu().numpy()
+    assert rel <= 1e-10
+    assert np.linalg.norm(b - As @ xh) / np.linalg.norm(b) < 1e-9  # true residual
+    xd = spla.spsolve(As.tocsc(), b)
+    assert np.linalg.norm(xh - xd) / np.linalg.norm(xd) < 1e-7
+    _, it_np = numpy_cg(As, b, 1e-10, 5000)
+    assert abs(it - it_np) <= 2
+    # bitwise reproducible, and check_every only changes where it stops
+    x2, it2, _ = S.cg(A, torch.as_tensor(b).cuda(), rtol=1e-10, max_iter=5000, check_every=1)
+    assert it2 == it and torch.equal(x, x2)
+    x3, it3, rel3 = S.cg(A, torch.as_tensor(b).cuda(), rtol=1e-10, max_iter=5000, check_every=16)
+    assert it <= it3 < it + 16 and rel3 <= 1e-10
+
+
+def test_cg_fp32_and_initial_guess():
+    m, n, Rst, Col, Val = laplace(64, 0.25)
+    A = R.spMtxCRS.from_host(m, n, Rst, Col, Val.astype(np.float32), dtype=torch.float32)
+    b = W.vector(n, 3).astype(np.float32)
+    x, it, rel = S.cg(A, torch.as_tensor(b).cuda(), rtol=1e-5, max_iter=2000, check_every=4)
+    As = sp.csr_matrix((Val, Col, Rst), shape=(m, n))
+    assert rel <= 1e-5
+    assert np.linalg.norm(b - As @ x.double().cpu().numpy()) / np.linalg.norm(b) < 1e-4
+    # starting from the solution: no iteration needed
+    _, it0, rel0 = S.cg(A, torch.as_tensor(b).cuda(), x0=x, rtol=1e-3, max_iter=10, check_every=1)
+    assert it0 == 0 and rel0 <= 1e-3
+
+
+def test_cg_max_iter_and_errors():
+    m, n, Rst, Col, Val = laplace(64)
+    A = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
+    b = torch.as_tensor(W.vector(n, 1)).cuda()
+    _, it, rel = S.cg(A, b, rtol=1e-14, max_iter=5, check_every=3)
+    assert it == 5 and rel > 1e-14
+    lib = R.load()
+    import ctypes as C
+    d = A.desc()  # no plan
+    it_, rr_ = C.c_int64(), C.c_double()
+    x = torch.zeros_like(b)
+    assert lib.rvvla_cg_f64(C.byref(d), b.data_ptr(), x.data_ptr(), 10, 1e-8, 1, C.byref(it_), C.byref(rr_),
+                            torch.cuda.current_stream().cuda_stream) != 0
+    m2, n2, R2, C2, V2 = W.random_rows(100, 80, "geometric", 0.2, "normal", seed=2)
+    A2 = R.spMtxCRS.from_host(m2, n2, R2, C2, V2, dtype=torch.float64)
+    with pytest.raises(ValueError):
+        S.cg(A2, torch.zeros(m2, dtype=torch.float64, device="cuda"))
