@@ -231,10 +231,10 @@ __device__ __forceinline__ auto hprod(V v, X x) {
 // The block-row's prefixes, block starts and row_ptr offsets are staged in
 // shared memory first, so an item's loads depend on no other global load; an
 // item issues the loads of kHcsrU chunks of 32 nonzeros before using any.
-constexpr int kHcsrThreads = 256;
+constexpr int kHcsrThreads = 512;
 constexpr int kHcsrWarps = kHcsrThreads / 32;
 constexpr int kHcsrU = 8;
-constexpr int kHcsrSlots = 8;  // loads in flight per lane in a CSR item
+constexpr int kHcsrSlots = 4;  // loads in flight per lane in a CSR item
 
 // 32 rows of a CSR block (local rows li0.., nr of them), G = 2^LG lanes per
 // row: a group strides through its row's contiguous nonzeros, so one warp
