@@ -604,6 +604,13 @@ int rvvla_cg_f64(const rvvla_crs* A, const double* b, double* x, int64_t max_ite
                  int64_t check_every, int64_t* iters, double* rel_res, void* stream);
 int rvvla_cg_f32(const rvvla_crs* A, const float* b, float* x, int64_t max_iter, double rtol,
                  int64_t check_every, int64_t* iters, double* rel_res, void* stream);
+/* y = A x and *dot = x^T A x (a device scalar) in one pass over A: the
+ * building block of the solver for other Krylov methods.  A square with an
+ * rvvla_crs_analyze plan (or without nonzeros: y = 0, *dot = 0); the dot
+ * is summed in a fixed order (bitwise reproducible); stream-ordered scratch
+ * of one value per 256-2048 nonzeros. */
+int rvvla_crs_spmv_dot_f64(const rvvla_crs* A, const double* x, double* y, double* dot, void* stream);
+int rvvla_crs_spmv_dot_f32(const rvvla_crs* A, const float* x, float* y, float* dot, void* stream);
 
 /* ------------------------------------------------------------ workloads
  * Seeded synthetic matrices on the host (OpenMP), written into caller

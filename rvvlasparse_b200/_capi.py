@@ -261,6 +261,8 @@ def load():
     _proto(lib, "rvvla_gen_vector", None, i64, u64, cint, dbl, dbl, vp)
     _proto(lib, "rvvla_cg_f64", cint, P(rvvla_crs), vp, vp, i64, dbl, i64, P(i64), P(dbl), vp)
     _proto(lib, "rvvla_cg_f32", cint, P(rvvla_crs), vp, vp, i64, dbl, i64, P(i64), P(dbl), vp)
+    _proto(lib, "rvvla_crs_spmv_dot_f64", cint, P(rvvla_crs), vp, vp, vp, vp)
+    _proto(lib, "rvvla_crs_spmv_dot_f32", cint, P(rvvla_crs), vp, vp, vp, vp)
     cp = C.c_char_p
     _proto(lib, "rvvla_host_crs_free", None, P(rvvla_host_crs))
     _proto(lib, "rvvla_mm_read", cint, cp, P(rvvla_host_crs))

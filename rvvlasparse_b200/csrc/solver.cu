@@ -122,6 +122,36 @@ __global__ void __launch_bounds__(kUpdThreads) cg_update_kernel(int64_t n, T* __
 }
 
 template <class T>
+__global__ void __launch_bounds__(kRedThreads) sum_to_kernel(const T* __restrict__ part, int64_t n, T* out) {
+  const double v = block_sum(part, n);
+  if (threadIdx.x == 0) *out = (T)v;
+}
+
+template <class T>
+int spmv_dot_impl(const rvvla_crs* A, const T* x, T* y, T* dot, cudaStream_t st) {
+  if (!A || !x || !y || !dot) return fail(RVVLA_ERR_INVALID_ARG, "crs_spmv_dot: null argument");
+  if (A->m != A->n) return fail(RVVLA_ERR_INVALID_ARG, "crs_spmv_dot: A must be square");
+  if (A->m == 0 || A->nz == 0) {  // y = 0, dot = 0
+    if (A->m > 0) RVVLA_CUDA(cudaMemsetAsync(y, 0, (size_t)A->m * sizeof(T), st));
+    RVVLA_CUDA(cudaMemsetAsync(dot, 0, sizeof(T), st));
+    return RVVLA_OK;
+  }
+  const int64_t nw = crs_warp_count(A->nz);
+  Scratch sc;
+  RVVLA_CUDA(sc.alloc((size_t)nw * sizeof(T), st));
+  int64_t np = 0;
+  const int rc = std::is_same<T, double>::value
+                     ? crs_spmv_dot_f64(A, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y),
+                                        sc.as<double>(), nw, &np, st)
+                     : crs_spmv_dot_f32(A, reinterpret_cast<const float*>(x), reinterpret_cast<float*>(y),
+                                        sc.as<float>(), nw, &np, st);
+  if (rc) return rc;
+  sum_to_kernel<T><<<1, kRedThreads, 0, st>>>(sc.as<T>(), np, dot);
+  RVVLA_LAUNCHED("sum_to_kernel");
+  return RVVLA_OK;
+}
+
+template <class T>
 __global__ void cg_p_kernel(int64_t n, T* __restrict__ p, const T* __restrict__ r, const CgScalars* __restrict__ s) {
   const T beta = (T)s->beta;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -221,6 +251,14 @@ int rvvla_cg_f64(const rvvla_crs* A, const double* b, double* x, int64_t max_ite
 int rvvla_cg_f32(const rvvla_crs* A, const float* b, float* x, int64_t max_iter, double rtol, int64_t check_every,
                  int64_t* iters, double* rel_res, void* stream) {
   return cg_impl<float>(A, b, x, max_iter, rtol, check_every, iters, rel_res, as_stream(stream));
+}
+
+int rvvla_crs_spmv_dot_f64(const rvvla_crs* A, const double* x, double* y, double* dot, void* stream) {
+  return spmv_dot_impl<double>(A, x, y, dot, as_stream(stream));
+}
+
+int rvvla_crs_spmv_dot_f32(const rvvla_crs* A, const float* x, float* y, float* dot, void* stream) {
+  return spmv_dot_impl<float>(A, x, y, dot, as_stream(stream));
 }
 
 }  // extern "C"

@@ -4,7 +4,7 @@ for symmetric positive definite matrices; the reference has no solver.
 Each iteration runs q = A p with p.q fused into the SpMV (the CRS lane-run
 kernel dots every row piece with p as it leaves the kernel), then the x / r
 update with the new r.r fused into the same pass; the host reads r.r every
-``check_every`` iterations.
+``check_every`` iterations.  ``spmv_dot`` exposes the fused product alone.
 """
 from __future__ import annotations
 
@@ -38,3 +38,21 @@ def cg(A: F.spMtxCRS, b: torch.Tensor, x0: torch.Tensor | None = None, rtol: flo
         msg = lib.rvvla_last_error().decode()
         raise (ValueError if st == _capi.RVVLA_ERR_INVALID_ARG else RuntimeError)(msg)
     return x, it.value, rr.value
+
+
+def spmv_dot(A: F.spMtxCRS, x: torch.Tensor):
+    """(y, d) with y = A x and d = x^T A x (a one-element CUDA tensor), in one
+    pass over A (square, fp64 or fp32)."""
+    if x.dtype != A.dtype or not x.is_cuda or x.numel() != A.n:
+        raise ValueError("spmv_dot: x must be a CUDA vector of A's type with n entries")
+    lib = _capi.load()
+    code = _capi.RVVLA_F64 if A.dtype == torch.float64 else _capi.RVVLA_F32
+    d = A.desc(code)
+    y = torch.empty(A.m, dtype=A.dtype, device=x.device)
+    dot = torch.empty(1, dtype=A.dtype, device=x.device)
+    fn = lib.rvvla_crs_spmv_dot_f64 if A.dtype == torch.float64 else lib.rvvla_crs_spmv_dot_f32
+    st = fn(C.byref(d), x.contiguous().data_ptr(), y.data_ptr(), dot.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    if st != 0:
+        msg = lib.rvvla_last_error().decode()
+        raise (ValueError if st == _capi.RVVLA_ERR_INVALID_ARG else RuntimeError)(msg)
+    return y, dot

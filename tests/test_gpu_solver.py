@@ -94,3 +94,30 @@ def test_cg_max_iter_and_errors():
     A2 = R.spMtxCRS.from_host(m2, n2, R2, C2, V2, dtype=torch.float64)
     with pytest.raises(ValueError):
         S.cg(A2, torch.zeros(m2, dtype=torch.float64, device="cuda"))
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_spmv_dot_fused(dt):
+    # y = A x and x^T A x in one pass, on matrices with and without empty rows
+    for empty in (False, True):
+        m, n, Rst, Col, Val = W.powerlaw(1 << 16, seed=9)
+        if empty:
+            ln = np.diff(Rst).astype(np.int64)
+            drop = np.arange(m) % 7 == 0
+            keep = np.repeat(~drop, ln)
+            ln[drop] = 0
+            Rst = np.concatenate([[0], np.cumsum(ln)]).astype(np.int32)
+            Col, Val = Col[keep], Val[keep]
+        tdt = torch.float64 if dt == np.float64 else torch.float32
+        A = R.spMtxCRS.from_host(m, n, Rst, Col, Val.astype(dt), dtype=tdt)
+        x = torch.as_tensor(W.vector(n, 4).astype(dt)).cuda()
+        y, d = S.spmv_dot(A, x)
+        As = sp.csr_matrix((Val.astype(np.float64), Col, Rst), shape=(m, n))
+        xh = x.double().cpu().numpy()
+        yref = As @ xh
+        tol = 1e-12 if dt == np.float64 else 1e-5
+        assert np.linalg.norm(y.double().cpu().numpy() - yref) / np.linalg.norm(yref) < tol
+        dref = xh @ yref
+        assert abs(float(d.item()) - dref) / abs(dref) < (1e-11 if dt == np.float64 else 1e-4)
+        y2, d2 = S.spmv_dot(A, x)
+        assert torch.equal(y, y2) and torch.equal(d, d2)
