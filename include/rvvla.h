@@ -262,6 +262,7 @@ typedef struct rvvla_lav_owned {
   void* sp_Val;
   uint32_t* row_order;
   uint8_t* lane_of_slot;
+  int32_t* sp_plan; /* rvvla_crs_analyze plan of sparse_part (the builder sets h.sparse_part.plan) */
 } rvvla_lav_owned;
 
 /* Builder (the reference has none; built on the host, then uploaded): dense

@@ -94,7 +94,7 @@ class rvvla_lav(C.Structure):
 class rvvla_lav_owned(C.Structure):
     _fields_ = [("h", rvvla_lav), ("chunk_offsets", vp), ("chunk_offsets_full_mask", vp), ("segment_ptr", vp),
                 ("out_order", vp), ("mask", vp), ("val", vp), ("col_id", vp), ("sp_Rst", vp), ("sp_Col", vp),
-                ("sp_Val", vp), ("row_order", vp), ("lane_of_slot", vp)]
+                ("sp_Val", vp), ("row_order", vp), ("lane_of_slot", vp), ("sp_plan", vp)]
 
 
 class rvvla_vnec(C.Structure):

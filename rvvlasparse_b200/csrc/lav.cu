@@ -223,6 +223,15 @@ int lav_build_typed(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen
   h.sparse_part.m = m; h.sparse_part.n = src->n; h.sparse_part.nz = (int64_t)H.sCol.size();
   h.sparse_part.Rst = out->sp_Rst; h.sparse_part.Col = out->sp_Col; h.sparse_part.Val = out->sp_Val;
   h.sparse_part.plan = nullptr; h.sparse_part.plan_tiles = 0; h.sparse_part.plan_kind = 0;
+  if (h.sparse_part.nz > 0) {  // analyse the sparse part once for the CRS lane-run kernel
+    const int dt = sizeof(T) == 8 ? RVVLA_F64 : RVVLA_F32;
+    const int64_t plen = rvvla_crs_plan_len(m, h.sparse_part.nz, dt);
+    RVVLA_CUDA(cudaMalloc(&out->sp_plan, (size_t)std::max<int64_t>(plen, 1) * sizeof(int32_t)));
+    int64_t tiles = 0;
+    int32_t kind = 0;
+    if ((rc = rvvla_crs_analyze(&h.sparse_part, dt, out->sp_plan, &tiles, &kind, st))) return rc;
+    h.sparse_part.plan = out->sp_plan; h.sparse_part.plan_tiles = tiles; h.sparse_part.plan_kind = kind;
+  }
   RVVLA_CUDA(cudaStreamSynchronize(st));
   return RVVLA_OK;
 }
@@ -306,7 +315,7 @@ int rvvla_lav_build(const rvvla_crs* src, int val_bytes, int64_t simd_lanes, dou
 void rvvla_lav_free(rvvla_lav_owned* h) {
   if (!h) return;
   void* ptrs[] = {h->chunk_offsets, h->chunk_offsets_full_mask, h->segment_ptr, h->out_order, h->mask, h->val,
-                  h->col_id, h->sp_Rst, h->sp_Col, h->sp_Val, h->row_order, h->lane_of_slot};
+                  h->col_id, h->sp_Rst, h->sp_Col, h->sp_Val, h->row_order, h->lane_of_slot, h->sp_plan};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   std::memset(h, 0, sizeof(*h));

@@ -108,3 +108,26 @@ def test_lav_long_chunks(lanes, seglen):
         V.long_chunks = nl
         y = run(V, 0.75, x, -0.5, y0)
         assert O.normwise_relerr(y, yref) < tol_for(np.float64), nl
+
+
+def test_lav_c_abi_builder_carries_sparse_part_plan():
+    # the C ABI alone: the builder analyses the sparse part, so a caller that
+    # never touches Python plans still gets the CRS lane-run kernel
+    import ctypes as C
+    from rvvlasparse_b200 import _capi
+    m, n, Rst, Col, Val = W.powerlaw(1 << 16, seed=12)
+    A = R.spMtxCRS.from_host(m, n, Rst, Col, Val, dtype=torch.float64)
+    lib = R.load()
+    owned = _capi.rvvla_lav_owned()
+    st = torch.cuda.current_stream().cuda_stream
+    assert lib.rvvla_lav_build(C.byref(A.desc()), 8, 8, 0.2, 5000, C.byref(owned), st) == 0
+    try:
+        assert owned.h.sparse_part.nz > 0 and owned.h.sparse_part.plan and owned.h.sparse_part.plan_kind in (1, 2)
+        x, y0 = W.vector(n, 1), W.vector(m, 2)
+        y = dev(y0)
+        assert lib.rvvla_lav_spmv_f64(C.byref(owned.h), 0.5, dev(x).data_ptr(), -1.0, y.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+        yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 0.5, x, -1.0, y0)
+        assert O.normwise_relerr(y.cpu().numpy(), yref) < 1e-12
+    finally:
+        lib.rvvla_lav_free(C.byref(owned))
