@@ -225,7 +225,7 @@ __device__ __forceinline__ auto hprod(V v, X x) {
 //
 // Work items of a block-row: every CSR block gives ceil(rows/32) items of 32
 // rows (a lane sums one row of the block); all COO nonzeros of the block-row,
-// taken block after block, form one stream cut into items of 256 nonzeros (a
+// taken block after block, form one stream cut into items of 128 nonzeros (a
 // lane finds the block of each of its 4 nonzeros by a shuffle search over the
 // COO prefix).  Tiny COO blocks therefore share warps instead of idling them.
 // The block-row's prefixes, block starts and row_ptr offsets are staged in
@@ -233,7 +233,7 @@ __device__ __forceinline__ auto hprod(V v, X x) {
 // item issues the loads of kHcsrU chunks of 32 nonzeros before using any.
 constexpr int kHcsrThreads = 512;
 constexpr int kHcsrWarps = kHcsrThreads / 32;
-constexpr int kHcsrU = 8;
+constexpr int kHcsrU = 4;
 constexpr int kHcsrSlots = 4;  // loads in flight per lane in a CSR item
 
 // 32 rows of a CSR block (local rows li0.., nr of them), G = 2^LG lanes per
@@ -378,7 +378,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __rest
         }
       }
     } else {
-      // 256 COO nonzeros of the block-row (blocks taken in order): lane 0
+      // 128 COO nonzeros of the block-row (blocks taken in order): lane 0
       // finds the block of the first one, lanes hold the next 32 block
       // boundaries and a shuffle search places every nonzero.  Nonzeros of
       // a block are in row order, so each chunk of 32 is summed per run of
