@@ -235,6 +235,10 @@ constexpr int kHcsrThreads = 512;
 constexpr int kHcsrWarps = kHcsrThreads / 32;
 constexpr int kHcsrU = 4;
 constexpr int kHcsrSlots = 4;  // loads in flight per lane in a CSR item
+// Three CTAs per SM (at most 40 registers a thread; the few spills stay in
+// L1): more block rows in flight hides the gather latency better than the
+// registers a two-CTA limit would leave.
+constexpr int kHcsrMinBlocks = 3;
 
 // 32 rows of a CSR block (local rows li0.., nr of them), G = 2^LG lanes per
 // row: a group strides through its row's contiguous nonzeros, so one warp
@@ -290,7 +294,7 @@ __device__ __forceinline__ void hcsr_csr_item(int rs, int e_beg, int e_end, int 
 }
 
 template <class V, class X, class SA, bool MIX>
-__global__ void __launch_bounds__(kHcsrThreads)
+__global__ void __launch_bounds__(kHcsrThreads, kHcsrMinBlocks)
 hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __restrict__ block_ptr,
                  const uint32_t* __restrict__ row_offset, const uint32_t* __restrict__ row_ptr,
                  const uint16_t* __restrict__ col_idx, const V* __restrict__ values, const X* __restrict__ x,
