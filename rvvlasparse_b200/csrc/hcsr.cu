@@ -235,10 +235,13 @@ constexpr int kHcsrThreads = 512;
 constexpr int kHcsrWarps = kHcsrThreads / 32;
 constexpr int kHcsrU = 4;
 constexpr int kHcsrSlots = 4;  // loads in flight per lane in a CSR item
-// Three CTAs per SM (at most 40 registers a thread; the few spills stay in
-// L1): more block rows in flight hides the gather latency better than the
-// registers a two-CTA limit would leave.
-constexpr int kHcsrMinBlocks = 3;
+// CTAs per SM the register budget is set for.  With 8-byte accumulators
+// (fp64, and the compensated pair of the mixed forms) three CTAs (at most 40
+// registers a thread; the few spills stay in L1) hide the gather latency
+// better than the registers a two-CTA limit would leave; plain fp32 sums
+// measured faster at two.
+template <class SA>
+constexpr int hcsr_min_blocks() { return sizeof(SA) == 8 ? 3 : 2; }
 
 // 32 rows of a CSR block (local rows li0.., nr of them), G = 2^LG lanes per
 // row: a group strides through its row's contiguous nonzeros, so one warp
@@ -294,7 +297,7 @@ __device__ __forceinline__ void hcsr_csr_item(int rs, int e_beg, int e_end, int 
 }
 
 template <class V, class X, class SA, bool MIX>
-__global__ void __launch_bounds__(kHcsrThreads, kHcsrMinBlocks)
+__global__ void __launch_bounds__(kHcsrThreads, hcsr_min_blocks<SA>())
 hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t b_n, const int* __restrict__ block_ptr,
                  const uint32_t* __restrict__ row_offset, const uint32_t* __restrict__ row_ptr,
                  const uint16_t* __restrict__ col_idx, const V* __restrict__ values, const X* __restrict__ x,
