@@ -772,7 +772,9 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 50 on the GPU arm, so each case's median is over 50 launches; "
+                         "20 on the reference arm, whose steps take seconds)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="powerlaw", choices=["powerlaw", "stencil", "laplace"])
@@ -784,6 +786,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the precision (stencil), batched and adjoint forms reported under 'forms'")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.impl == "reference" else 50
+    if args.steps < 1:
+        ap.error("--steps must be >= 1")
     if args.impl == "reference":
         run_reference(args)
     else:
