@@ -424,7 +424,16 @@ def _lav_convert(dist, src: spMtxCRS, params: convertParams) -> None:
 
 class spMtxVHCC(_GpuFormat):
     """``spMtxVHCC<ValT>`` (include/VHCC.h:43-62): the underscore fields of
-    the reference without the underscore, vhcc_params flattened."""
+    the reference without the underscore, vhcc_params flattened.
+
+    ``num_panels`` > 1 (vhcc_params, include/VHCC.h:15-26; the reference
+    stores it, but its only kernel, vhcc_spmv_1panel_riscv in
+    src/rvv/spmv_vhcc.cpp:73, runs one panel): the columns are cut into
+    contiguous ranges of about nz / num_panels nonzeros, ``panels`` holds one
+    single-panel spMtxVHCC per non-empty range (global column indices kept),
+    and a product runs them in order — β on the first, 1 after — so row i
+    sums its panels' partial sums in column-range order.  The object itself
+    then holds only the scalars."""
 
     SCALARS = ("num_rows", "num_cols", "num_entries", "num_vectors", "pad_entries", "pad_rows", "num_threads",
                "num_panels", "tile_row", "tile_col", "vec_size", "n_masks", "n_eor", "scan_mask_bytes", "n_rowarr")
@@ -433,8 +442,93 @@ class spMtxVHCC(_GpuFormat):
     CDESC = _capi.rvvla_vhcc
     VALUE = "vals_arr"
 
+    def __init__(self):
+        super().__init__()
+        self.panels: list[spMtxVHCC] = []
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return self.panels[0].dtype if self.panels else super().dtype
+
+    def astype(self, dtype: torch.dtype):
+        if not self.panels:
+            return super().astype(dtype)
+        c = type(self)()
+        c.__dict__.update(self.__dict__)
+        c.panels = [p.astype(dtype) for p in self.panels]
+        return c
+
+    def desc(self):
+        if self.panels:
+            raise ValueError("spMtxVHCC: a multi-panel matrix has one descriptor per panel (.panels[k].desc())")
+        return super().desc()
+
+    def to_host(self) -> dict:
+        if not self.panels:
+            return super().to_host()
+        out = {k: int(getattr(self, k)) for k in self.SCALARS}
+        out["panels"] = [p.to_host() for p in self.panels]
+        return out
+
+
+def column_panels(src: spMtxCRS, num_panels: int) -> list[tuple[int, int, spMtxCRS]]:
+    """Cuts ``src`` by columns into ``num_panels`` contiguous ranges [c0, c1)
+    holding about nz / num_panels nonzeros each (whole columns, so a range
+    may hold more, or nothing), as (c0, c1, CRS of the same shape with only
+    that range's nonzeros, global column indices, row-major order kept).
+    Torch operations on the arrays' own device; the multi-panel VHCC
+    builder's split."""
+    P = int(num_panels)
+    if P < 1:
+        raise ValueError("column_panels: num_panels must be >= 1")
+    m, n, nz = src.m, src.n, src.nz
+    dev = src.Col.device
+    col = src.Col[:nz].long()
+    prefix = torch.zeros(n + 1, dtype=torch.int64, device=dev)  # nonzeros in columns < c
+    if nz:
+        prefix[1:] = torch.cumsum(torch.bincount(col, minlength=n)[:n], 0)
+    targets = (torch.arange(1, P, dtype=torch.int64, device=dev) * nz) // P
+    inner = torch.searchsorted(prefix, targets, side="left").clamp(0, n)
+    bounds = torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), inner,
+                        torch.full((1,), n, dtype=torch.int64, device=dev)])
+    bounds = torch.cummax(bounds, 0).values.tolist()
+    row_of = torch.repeat_interleave(torch.arange(m, device=dev), torch.diff(src.Rst.long()), output_size=nz)
+    out = []
+    for k in range(P):
+        c0, c1 = int(bounds[k]), int(bounds[k + 1])
+        keep = (col >= c0) & (col < c1)
+        cnt = torch.bincount(row_of[keep], minlength=m)[:m]
+        Rst = torch.zeros(m + 1, dtype=torch.int32, device=dev)
+        Rst[1:] = torch.cumsum(cnt, 0).to(torch.int32)
+        Col, Val = src.Col[:nz][keep].contiguous(), src.Val[:nz][keep].contiguous()
+        out.append((c0, c1, spMtxCRS(m, n, int(Col.numel()), Rst, Col, Val)))
+    return out
+
 
 def _vhcc_convert(dist, src: spMtxCRS, params: convertParams) -> None:
+    P = int(params.param.get("num_panels", 1))
+    if P < 1:
+        raise ValueError("convert<spMtxVHCC>: num_panels must be >= 1")
+    if P > 1 and src.nz > 0:
+        one = convertParams({k: v for k, v in params.param.items() if k != "num_panels"})
+        parts = []
+        for _, _, sub in column_panels(src, P):
+            if sub.nz:
+                parts.append(spMtxVHCC())
+                _vhcc_convert(parts[-1], sub, one)
+        head = parts[0]
+        for k in spMtxVHCC.SCALARS:
+            setattr(dist, k, getattr(head, k))
+        for k in spMtxVHCC.ARRAYS:
+            setattr(dist, k, None)
+        dist.num_panels = len(parts)
+        dist.num_entries = src.nz
+        for k in ("num_vectors", "pad_entries", "n_eor", "scan_mask_bytes", "n_rowarr", "num_threads"):
+            setattr(dist, k, sum(int(getattr(q, k)) for q in parts))
+        dist.pad_rows = max(int(q.pad_rows) for q in parts)
+        dist.panels = parts
+        return
+    dist.panels = []
     lib = load()
     owned = _capi.rvvla_vhcc_owned()
     nt = int(params.param.get("num_threads", 0))
@@ -581,7 +675,13 @@ def _call_spmv(mat, alpha, b: torch.Tensor, beta, y: torch.Tensor, mixed: bool,
         if mixed:
             return _capi.RVVLA_ERR_UNSUPPORTED
         fn = lib.rvvla_vhcc_spmv_f64 if vt == torch.float64 else lib.rvvla_vhcc_spmv_f32
-        return fn(C.byref(mat.desc()), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        if not mat.panels:
+            return fn(C.byref(mat.desc()), float(alpha), _ptr(b), float(beta), _ptr(y), st)
+        for k, p in enumerate(mat.panels):  # y = alpha * A_k b + (beta, then 1) * y, panel after panel
+            rc = fn(C.byref(p.desc()), float(alpha), _ptr(b), float(beta) if k == 0 else 1.0, _ptr(y), st)
+            if rc:
+                return rc
+        return 0
     if isinstance(mat, spMtxVNEC):
         if mixed:
             return _capi.RVVLA_ERR_UNSUPPORTED

@@ -121,6 +121,8 @@ def _state(obj) -> dict:
             fields[k] = ("value", v)
         elif type(v).__name__ in _CLASSES:
             fields[k] = ("format", _state(v))
+        elif isinstance(v, list) and all(type(e).__name__ in _CLASSES for e in v):  # multi-panel VHCC
+            fields[k] = ("formats", [_state(e) for e in v])
         else:
             raise TypeError(f"save_format: field {k} of {type(obj).__name__} cannot be stored ({type(v).__name__})")
     return {"class": type(obj).__name__, "fields": fields}
@@ -136,6 +138,8 @@ def _restore(state: dict, device):
             v = v.to(device)
         elif kind == "format":
             v = _restore(v, device)
+        elif kind == "formats":
+            v = [_restore(e, device) for e in v]
         setattr(obj, k, v)
     return obj
 
