@@ -1,6 +1,5 @@
 """GPU: every built format survives save_format / load_format (arrays equal,
 same SpMV result), including a bf16-valued mixed-precision copy."""
-import numpy as np
 import pytest
 import torch
 

@@ -1,7 +1,5 @@
 """On-disk formats: the native Matrix Market reader/writer and the binary
 CRS container (CPU only)."""
-import os
-
 import numpy as np
 import pytest
 

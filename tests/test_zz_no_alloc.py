@@ -3,7 +3,6 @@ scratch) against the ordinary one, called through the C ABI.  Collected
 last so that it also runs after every other GPU test in the session."""
 import ctypes as C
 
-import numpy as np
 import pytest
 import torch
 
