@@ -211,8 +211,6 @@ __device__ __forceinline__ int warp_count_le(int b, int q) {
 
 template <class V>
 __device__ __forceinline__ V ldval(const V* p, uint64_t pol) { return ld_stream(p, pol); }
-template <>
-__device__ __forceinline__ __nv_bfloat16 ldval<__nv_bfloat16>(const __nv_bfloat16* p, uint64_t) { return ldv(p); }
 
 template <bool MIX, class V, class X>
 __device__ __forceinline__ auto hprod(V v, X x) {
@@ -235,11 +233,11 @@ constexpr int kHcsrThreads = 512;
 constexpr int kHcsrWarps = kHcsrThreads / 32;
 constexpr int kHcsrU = 4;
 constexpr int kHcsrSlots = 4;  // loads in flight per lane in a CSR item
-// CTAs per SM the register budget is set for.  With 8-byte accumulators
-// (fp64, and the compensated pair of the mixed forms) three CTAs (at most 40
-// registers a thread; the few spills stay in L1) hide the gather latency
-// better than the registers a two-CTA limit would leave; plain fp32 sums
-// measured faster at two.
+// CTAs per SM the register budget is set for.  With 8-byte shared
+// accumulators (fp64, and the fp64 merge of the mixed forms) three CTAs (at
+// most 40 registers a thread; the few spills stay in L1) hide the gather
+// latency better than the registers a two-CTA limit would leave; plain fp32
+// sums measured faster at two.
 template <class SA>
 constexpr int hcsr_min_blocks() { return sizeof(SA) == 8 ? 3 : 2; }
 
