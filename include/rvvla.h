@@ -384,7 +384,11 @@ typedef struct rvvla_vhcc_owned {
 
 /* Builder (the reference has only setters, include/VHCC.h:80-112): one
  * panel, vec_size 32 (one vector lane per warp lane), num_threads equal
- * vector ranges (<= 0: 64 vectors each).  Synchronises `stream`. */
+ * vector ranges (<= 0: 64 vectors each).  Synchronises `stream`.
+ * Several panels (vhcc_params.num_panels, include/VHCC.h:15-26): build one
+ * structure per column range of the CRS (global column indices kept) and
+ * call rvvla_vhcc_spmv_* on them in column order, beta on the first and 1
+ * after; the Python mirror does this for convertParams(num_panels=P). */
 int rvvla_vhcc_build(const rvvla_crs* src, int val_bytes, int64_t num_threads, rvvla_vhcc_owned* out,
                      void* stream);
 void rvvla_vhcc_free(rvvla_vhcc_owned* h);
