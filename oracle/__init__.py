@@ -8,6 +8,10 @@ Two libraries, both built by ``oracle/Makefile``:
   (RVVLASparse src/scalar/*.cpp) compiled where they lie, behind the
   ``extern "C"`` shim ref_shim.cpp.  Built only where the reference sources
   are present; the built file travels with the repository snapshot.
+* ``_ref/libref_rvv.so`` — the reference's RVV-only kernels (CSR5, VNEC,
+  VHCC: src/rvv/spmv_mtx_csr5.cpp, spmv_mtx_vnec.cpp, spmv_vhcc.cpp) compiled
+  where they lie against the scalar intrinsic stand-in
+  ``rvv_emul/riscv_vector.h`` (VLEN 256), behind the shim rvv_shim.cpp.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` may import this package, and only as the checker / the timed CPU
@@ -24,6 +28,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_scalar.so")
+REFV_LIB = os.path.join(HERE, "_ref", "libref_rvv.so")
 REF_SRC = os.environ.get("RVVLA_REFERENCE_SRC", "/root/reference")
 
 I32, U32, U16, U8, F32, F64, I64, U64 = range(8)
@@ -33,10 +38,12 @@ _CODE = {np.dtype(v): k for k, v in _NP.items()}
 
 _olib = None
 _rlib = None
+_vlib = None
 
 
 def build(ref: bool = True) -> None:
-    """make -C oracle (and the reference library when its sources exist)."""
+    """make -C oracle (and the reference libraries, scalar and RVV, when its
+    sources exist)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True, capture_output=True)
     if ref and os.path.isdir(os.path.join(REF_SRC, "src", "scalar")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True, capture_output=True)
@@ -429,6 +436,146 @@ def ref_cvr(b: Bundle) -> RefMatrix:
     h = getattr(L, f"refx_cvr_new_{_sfx(dt)}")(ints.ctypes.data, lens.ctypes.data, vals.ctypes.data,
                                                cols.ctypes.data, rec.ctypes.data, wb.ctypes.data)
     return RefMatrix("cvr", h, dt)
+
+
+# ------------------------------------------------ reference RVV kernels
+def refv_available() -> bool:
+    return os.path.exists(REFV_LIB)
+
+
+def _refv():
+    global _vlib
+    if _vlib is None:
+        if not os.path.exists(REFV_LIB):
+            raise RuntimeError("reference RVV library not built (make -C oracle ref-rvv)")
+        L = C.CDLL(REFV_LIB)
+        vp, i64, dbl, flt, cint = C.c_void_p, C.c_int64, C.c_double, C.c_float, C.c_int
+        L.refv_last_error.restype = C.c_char_p
+        L.refv_num_threads.restype = cint
+        L.refv_vlen.restype = cint
+        for S, T in (("f64", dbl), ("f32", flt)):
+            def p(name, res, args):
+                f = getattr(L, name.replace("@", S))
+                f.restype, f.argtypes = res, args
+            p("refv_csr5_new_@", vp, [vp, vp, vp, vp, vp, vp, vp, vp, vp])
+            p("refv_csr5_free_@", None, [vp])
+            p("refv_csr5_spmv_@", cint, [vp, cint, T, vp, T, vp])
+            p("refv_vhcc_new_@", vp, [vp, vp, vp, vp, vp, vp, vp, vp])
+            p("refv_vhcc_free_@", None, [vp])
+            p("refv_vhcc_spmv_@", cint, [vp, T, vp, T, vp])
+            p("refv_vnec_new_@", vp, [i64, i64, i64, vp, vp, vp])
+            p("refv_vnec_free_@", None, [vp])
+            p("refv_vnec_info_@", None, [vp, vp, vp])
+            p("refv_vnec_spmv_@", cint, [vp, T, vp, T, vp])
+        _vlib = L
+    return _vlib
+
+
+def refv_vlen() -> int:
+    """VLEN (bits) of the intrinsic stand-in the RVV library was built with."""
+    return int(_refv().refv_vlen())
+
+
+def refv_lanes(sew: int, lmul: int) -> int:
+    """VLMAX for SEW-bit elements at LMUL on that VLEN."""
+    return refv_vlen() * lmul // sew
+
+
+class RefRvvMatrix:
+    """A matrix held by the reference RVV library (owning handle); spmv runs
+    the reference's sparse_mv<T, Fmt, true>."""
+
+    def __init__(self, kind: str, handle, dt, keep=()):
+        if not handle:
+            raise RuntimeError(_refv().refv_last_error().decode())
+        self.kind, self.h, self.dt, self._keep = kind, handle, np.dtype(dt), keep
+
+    def __del__(self):
+        try:
+            getattr(_refv(), f"refv_{self.kind}_free_{_sfx(self.dt)}")(self.h)
+        except Exception:
+            pass
+
+    def spmv(self, alpha, b, beta, y) -> np.ndarray:
+        b = _a(b, self.dt)
+        out = np.array(y, dtype=self.dt, copy=True)
+        fn = getattr(_refv(), f"refv_{self.kind}_spmv_{_sfx(self.dt)}")
+        if self.kind == "csr5":
+            rc = fn(self.h, self.threads, alpha, b.ctypes.data, beta, out.ctypes.data)
+        else:
+            rc = fn(self.h, alpha, b.ctypes.data, beta, out.ctypes.data)
+        assert rc == 0, rc
+        return out
+
+
+def refv_max_threads() -> int:
+    return int(_refv().refv_num_threads())
+
+
+def refv_csr5(b: Bundle, threads: int = 0) -> RefRvvMatrix:
+    """The reference's RVV CSR5 kernel (src/rvv/spmv_mtx_csr5.cpp:33-586) on
+    a layout from build_csr5; omega must equal a VLMAX of the stand-in
+    (e64 m1..m8 / e32 m1..m8), or the reference's entry asserts."""
+    dt = b.dtype
+    ints = np.array([b[k] for k in ("m", "n", "nnz", "bit_y_offset", "bit_seg_offset", "tile_desc_len",
+                                    "tail_tile_start", "p", "omega", "sigma", "num_offsets")], np.int64)
+    sew = 64 if dt == np.float64 else 32
+    if int(b["omega"]) not in [refv_lanes(sew, k) for k in (1, 2, 4, 8)]:
+        raise ValueError(f"refv_csr5: omega {int(b['omega'])} is no VLMAX of e{sew} at VLEN {refv_vlen()}")
+    rp, col, val = _a(b["csr_row_pointer"], np.int32), _a(b["csr_column_index"], np.uint32), _a(b["csr_value"], dt)
+    tp, td = _a(b["tile_pointer"], np.uint32), _a(b["tile_descriptor"], np.uint32)
+    tep, te = _a(b["tile_empty_offset_pointer"], np.uint32), _a(b["tile_empty_offset"], np.uint32)
+    lens = np.array([len(rp), len(col), len(tp), len(td), len(tep), len(te)], np.int64)
+    h = getattr(_refv(), f"refv_csr5_new_{_sfx(dt)}")(ints.ctypes.data, lens.ctypes.data, rp.ctypes.data,
+                                                      col.ctypes.data, val.ctypes.data, tp.ctypes.data,
+                                                      td.ctypes.data, tep.ctypes.data, te.ctypes.data)
+    mat = RefRvvMatrix("csr5", h, dt)
+    # With fewer full tiles than OpenMP threads the reference's CSR5 gives wrong
+    # sums in a few per cent of calls (a race in its tile split, observed on
+    # 4-tile matrices with 8 threads and never at 1-2 threads or at >= 6 tiles a
+    # thread); it runs here with at least 8 full tiles a thread unless told.
+    mat.threads = int(threads) if threads else max(1, min(refv_max_threads(), (int(b["p"]) - 1) // 8))
+    return mat
+
+
+def refv_vhcc(b: Bundle) -> RefRvvMatrix:
+    """The reference's RVV VHCC kernel (src/rvv/spmv_vhcc.cpp:27-434) on a
+    layout from build_vhcc; vec_size must be the kernel's vector length
+    (e64m2 / e32m2 VLMAX: 8 fp64 / 16 fp32 at VLEN 256)."""
+    dt = b.dtype
+    sew = 64 if dt == np.float64 else 32
+    if int(b["vec_size"]) != refv_lanes(sew, 2):
+        raise ValueError(f"refv_vhcc: vec_size must be {refv_lanes(sew, 2)} for e{sew}m2")
+    ints = np.array([b[k] for k in ("num_rows", "num_cols", "num_entries", "num_vectors", "pad_entries",
+                                    "pad_rows", "num_threads", "vec_size")], np.int64)
+    thr, veo = _a(b["thr_info"], np.int32), _a(b["veceor_ptr"], np.uint32)
+    sm = np.ascontiguousarray(b["scan_mask"]).view(np.uint8)
+    ra, ca, va = _a(b["row_arr"], np.uint32), _a(b["col_arr"], np.uint32), _a(b["vals_arr"], dt)
+    lens = np.array([len(thr), len(veo), len(sm), len(ra), len(ca)], np.int64)
+    h = getattr(_refv(), f"refv_vhcc_new_{_sfx(dt)}")(ints.ctypes.data, lens.ctypes.data, thr.ctypes.data,
+                                                      veo.ctypes.data, sm.ctypes.data, ra.ctypes.data,
+                                                      ca.ctypes.data, va.ctypes.data)
+    return RefRvvMatrix("vhcc", h, dt, keep=(thr, veo, sm, ra, ca, va))
+
+
+def refv_vnec(src: Bundle) -> RefRvvMatrix:
+    """The reference's own VNEC (constructor include/VNEC.h:200-227, kernels
+    src/rvv/spmv_mtx_vnec.cpp:18-738) on a CRS; ``.info()`` gives the variant
+    it chose (0 D, 1 S, 2 L), its thread count and IRD."""
+    dt = src.dtype
+    R, Cc, V = _a(src["Rst"], np.int32), _a(src["Col"], np.int32), _a(src["Val"], dt)
+    h = getattr(_refv(), f"refv_vnec_new_{_sfx(dt)}")(int(src["m"]), int(src["n"]), int(src["nz"]), R.ctypes.data,
+                                                      Cc.ctypes.data, V.ctypes.data)
+    mat = RefRvvMatrix("vnec", h, dt, keep=(R, Cc, V))
+
+    def info():
+        out = np.zeros(2, np.int64)
+        ird = C.c_double()
+        getattr(_refv(), f"refv_vnec_info_{_sfx(dt)}")(mat.h, out.ctypes.data, C.byref(ird))
+        return {"vnec_t": int(out[0]), "threads": int(out[1]), "IRD_mat": float(ird.value)}
+
+    mat.info = info
+    return mat
 
 
 def ref_num_threads() -> int:

@@ -7,15 +7,20 @@
 //     pinned: tests compare them against the reference scalar library compiled
 //     from its own sources (oracle/_ref) and against tests/golden/ fixtures it
 //     wrote.
-//   * CSR5, VNEC (S/D/L) and VHCC SpMV exist in the reference only as RVV
-//     intrinsics (src/rvv/), which cannot be compiled here.  They are restated
-//     from those files and pinned only indirectly, against the long-double CSR
-//     result on the same matrix ("parity unpinned" by the reference itself).
+//   * CSR5 and VHCC SpMV exist in the reference only as RVV intrinsics
+//     (src/rvv/).  Those files compile unmodified against the scalar
+//     intrinsic stand-in rvv_emul/riscv_vector.h (oracle/_ref/libref_rvv.so),
+//     and tests run them on this oracle's layouts: both are pinned.
+//   * VNEC (S/D/L) SpMV is restated from src/rvv/spmv_mtx_vnec.cpp, whose
+//     kernels read structures no reference code fills; it is pinned only
+//     indirectly, against the long-double CSR result on the same matrix
+//     ("parity unpinned" by the reference itself).
 //   * The reference ships no builder for SELL-C-sigma, CSR5, LAV, VNEC S/D,
 //     VHCC or CVR.  The builders here define the layout each reference kernel
 //     reads; they are pinned by round trips (format -> CSR == source) and by
-//     the reference kernels run on their output (SELL, LAV, CVR via
-//     oracle/_ref).  Parity of those builders is unpinned by the reference.
+//     the reference kernels run on their output (SELL, LAV, CVR, CSR5, VHCC
+//     via oracle/_ref).  Parity of those builders is unpinned by the
+//     reference.
 //
 // All formats travel as a "bundle": a format tag, named typed arrays and named
 // scalars, so one ctypes binding serves every format.

@@ -1,0 +1,124 @@
+"""Pinning the oracle's CSR5 and VHCC restatements to the reference's own
+RVV-only kernels (src/rvv/spmv_mtx_csr5.cpp, src/rvv/spmv_vhcc.cpp), compiled
+unmodified for x86-64 against the scalar intrinsic stand-in
+oracle/rvv_emul/riscv_vector.h (VLEN 256) into oracle/_ref/libref_rvv.so.
+
+The reference has no builder for either format, so both sides run on the
+same layout from the oracle's builders; the reference computes with its own
+vector code (fused multiply-adds, its reductions, its thread split), so the
+check is normwise, at the restatement tolerances (1e-12 fp64, 1e-5 fp32),
+against the restatement and against the long-double CSR oracle.  Also
+pinned here: the stand-in's own semantics on small known cases."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import golden_files, golden_id, load_golden, tol_for
+from rvvlasparse_b200 import workloads as W
+
+pytestmark = pytest.mark.skipif(not O.refv_available(), reason="reference RVV library not built")
+GOLD = golden_files()
+
+
+@pytest.fixture(params=GOLD, ids=[golden_id(p) for p in GOLD])
+def g(request):
+    return load_golden(request.param)
+
+
+def omegas(dt):
+    sew = 64 if np.dtype(dt) == np.float64 else 32
+    return [O.refv_lanes(sew, k) for k in (1, 2, 4, 8)]
+
+
+def test_stand_in_vector_lengths():
+    assert O.refv_vlen() == 256
+    assert omegas(np.float64) == [4, 8, 16, 32] and omegas(np.float32) == [8, 16, 32, 64]
+
+
+@pytest.mark.parametrize("omega_sigma", [(32, 8), (32, 16), (32, 24), (32, 32), (16, 16), (8, 4)])
+def test_csr5_reference_kernel_golden(g, omega_sigma):
+    """The GPU path's tiles (omega 32, sigma 8..32) and smaller ones."""
+    omega, sigma = omega_sigma
+    dt = g["Val"].dtype
+    if omega not in omegas(dt):
+        pytest.skip(f"omega {omega} is no VLMAX for {dt}")
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    b = O.build_csr5(src, omega, sigma)
+    yr = O.refv_csr5(b).spmv(g["alpha"], g["x"], g["beta"], g["y0"])
+    yo = O.spmv(b, g["alpha"], g["x"], g["beta"], g["y0"])
+    yld = O.crs_spmv_ld(src, g["alpha"], g["x"], g["beta"], g["y0"])
+    assert O.normwise_relerr(yr, yo) < tol_for(dt)
+    assert O.normwise_relerr(yr, yld) < tol_for(dt)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_csr5_reference_kernel_powerlaw_all_omegas(dt):
+    m, n, R, C, V = W.powerlaw(3000, seed=3)
+    V = V.astype(dt)
+    src = O.crs(m, n, R, C, V)
+    x, y0 = W.vector(n, 0).astype(dt), W.vector(m, 1).astype(dt)
+    yld = O.crs_spmv_ld(src, 1.25, x, 0.5, y0)
+    for omega in omegas(dt):
+        for sigma in (4, 8, 16, 32):
+            if sigma > omega:
+                continue
+            b = O.build_csr5(src, omega, sigma)
+            yr = O.refv_csr5(b).spmv(1.25, x, 0.5, y0)
+            assert O.normwise_relerr(yr, O.spmv(b, 1.25, x, 0.5, y0)) < tol_for(dt), (omega, sigma)
+            assert O.normwise_relerr(yr, yld) < tol_for(dt), (omega, sigma)
+
+
+def test_csr5_reference_sigma_above_omega_skips_part_of_single_row_tiles():
+    """The reference passes (sigma, omega) to a simple-tile routine declared
+    (omega, sigma) (src/rvv/spmv_mtx_csr5.cpp:161-163 against :44-46): with
+    sigma > omega it asks for sigma lanes per step, gets omega (VLMAX), and
+    steps sigma elements, so a tile that lies inside one row loses part of its
+    sum.  The restatement sums the whole tile; the GPU path only uses
+    sigma <= omega = 32."""
+    g = load_golden([p for p in GOLD if "one_long_row_f64" in p][0])
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    b = O.build_csr5(src, 4, 16)
+    yld = O.crs_spmv_ld(src, g["alpha"], g["x"], g["beta"], g["y0"])
+    assert O.normwise_relerr(O.spmv(b, g["alpha"], g["x"], g["beta"], g["y0"]), yld) < 1e-12
+    assert O.normwise_relerr(O.refv_csr5(b).spmv(g["alpha"], g["x"], g["beta"], g["y0"]), yld) > 1e-3
+
+
+def test_csr5_reference_rejects_omega_without_vector_length():
+    m, n, R, C, V = W.powerlaw(500, seed=2)
+    b = O.build_csr5(O.crs(m, n, R, C, V), 12, 4)
+    with pytest.raises(ValueError):
+        O.refv_csr5(b)
+
+
+@pytest.mark.parametrize("threads", [1, 3, 8])
+def test_vhcc_reference_kernel_golden(g, threads):
+    dt = g["Val"].dtype
+    sew = 64 if dt == np.float64 else 32
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    b = O.build_vhcc(src, threads, O.refv_lanes(sew, 2))
+    ref = O.refv_vhcc(b)
+    for alpha, beta in ((g["alpha"], g["beta"]), (1.0, 0.0)):
+        yr = ref.spmv(alpha, g["x"], beta, g["y0"])
+        assert O.normwise_relerr(yr, O.spmv(b, alpha, g["x"], beta, g["y0"])) < tol_for(dt)
+        assert O.normwise_relerr(yr, O.crs_spmv_ld(src, alpha, g["x"], beta, g["y0"])) < tol_for(dt)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_vhcc_reference_kernel_powerlaw(dt):
+    m, n, R, C, V = W.powerlaw(3000, seed=3)
+    V = V.astype(dt)
+    src = O.crs(m, n, R, C, V)
+    x, y0 = W.vector(n, 0).astype(dt), W.vector(m, 1).astype(dt)
+    sew = 64 if dt == np.float64 else 32
+    for threads in (1, 3, 8):
+        b = O.build_vhcc(src, threads, O.refv_lanes(sew, 2))
+        for alpha, beta in ((1.25, 0.5), (1.0, 0.0), (-0.5, 2.0)):
+            yr = O.refv_vhcc(b).spmv(alpha, x, beta, y0)
+            assert O.normwise_relerr(yr, O.spmv(b, alpha, x, beta, y0)) < tol_for(dt)
+            assert O.normwise_relerr(yr, O.crs_spmv_ld(src, alpha, x, beta, y0)) < tol_for(dt)
+
+
+def test_vhcc_reference_rejects_other_vector_sizes():
+    m, n, R, C, V = W.powerlaw(500, seed=2)
+    with pytest.raises(ValueError):
+        O.refv_vhcc(O.build_vhcc(O.crs(m, n, R, C, V), 2, 32))
