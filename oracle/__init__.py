@@ -463,10 +463,11 @@ def _refv():
             p("refv_vhcc_new_@", vp, [vp, vp, vp, vp, vp, vp, vp, vp])
             p("refv_vhcc_free_@", None, [vp])
             p("refv_vhcc_spmv_@", cint, [vp, T, vp, T, vp])
-            p("refv_vnec_new_@", vp, [i64, i64, i64, vp, vp, vp])
+            p("refv_vnec_new_@", vp, [i64, i64, i64, vp, vp, vp, cint])
             p("refv_vnec_free_@", None, [vp])
             p("refv_vnec_info_@", None, [vp, vp, vp])
             p("refv_vnec_spmv_@", cint, [vp, T, vp, T, vp])
+            p("refv_vnec_fill_@", cint, [vp] * 20)
         _vlib = L
     return _vlib
 
@@ -558,15 +559,43 @@ def refv_vhcc(b: Bundle) -> RefRvvMatrix:
     return RefRvvMatrix("vhcc", h, dt, keep=(thr, veo, sm, ra, ca, va))
 
 
-def refv_vnec(src: Bundle) -> RefRvvMatrix:
+def refv_vnec(src: Bundle, layout: Bundle | None = None, threads: int = 0) -> RefRvvMatrix:
     """The reference's own VNEC (constructor include/VNEC.h:200-227, kernels
-    src/rvv/spmv_mtx_vnec.cpp:18-738) on a CRS; ``.info()`` gives the variant
-    it chose (0 D, 1 S, 2 L), its thread count and IRD."""
+    src/rvv/spmv_mtx_vnec.cpp:18-738) on a CRS; ``.info()`` gives the variant,
+    thread count and IRD (``threads``: the OpenMP team size the constructor
+    runs with; 0 = the default).  The reference fills none of the structures its
+    kernels read, so ``layout`` (a build_vnec bundle of the same matrix) is
+    needed before ``spmv``: its arrays, variant and thread count are set on
+    the reference object (rvv_shim.cpp, refv_vnec_fill)."""
     dt = src.dtype
     R, Cc, V = _a(src["Rst"], np.int32), _a(src["Col"], np.int32), _a(src["Val"], dt)
     h = getattr(_refv(), f"refv_vnec_new_{_sfx(dt)}")(int(src["m"]), int(src["n"]), int(src["nz"]), R.ctypes.data,
-                                                      Cc.ctypes.data, V.ctypes.data)
-    mat = RefRvvMatrix("vnec", h, dt, keep=(R, Cc, V))
+                                                      Cc.ctypes.data, V.ctypes.data, int(threads))
+    keep = [R, Cc, V]
+    mat = RefRvvMatrix("vnec", h, dt, keep=keep)
+    if layout is not None:
+        def arr(k, t):
+            if k not in layout.arrays:
+                return None
+            a = _a(layout[k], t)
+            keep.append(a)
+            return a
+
+        names = [("thread_coord_start", np.int32), ("thread_coord_end", np.int32), ("NEC_NUM", np.int32),
+                 ("use_x_ptr", np.int32), ("use_x_indices", np.int32), ("ecr_indices", np.int32),
+                 ("v_row_ptr", np.int32), ("col_start", np.int32), ("val_align", dt), ("tasks", np.int32),
+                 ("task_start", np.int32), ("task_end", np.int32), ("spvv_len", np.int32), ("row_begin", np.int32),
+                 ("row_end", np.int32), ("reorder_col", np.int32), ("reorder_nnz", dt)]
+        got = {k: arr(k, t) for k, t in names}
+        ln = lambda k: 0 if got[k] is None else len(got[k])  # noqa: E731
+        ints = np.array([int(layout["vnec_t"]), int(layout["NUM_THREADS_VNEC"])], np.int64)
+        lens = np.array([ln("ecr_indices"), ln("use_x_indices"), ln("v_row_ptr"), ln("col_start"), ln("val_align"),
+                         ln("tasks"), ln("row_begin"), ln("reorder_col")], np.int64)
+        keep += [ints, lens]
+        ptrs = [None if got[k] is None else got[k].ctypes.data for k, _ in names]
+        rc = getattr(_refv(), f"refv_vnec_fill_{_sfx(dt)}")(h, ints.ctypes.data, lens.ctypes.data, *ptrs)
+        if rc != 0:
+            raise RuntimeError(_refv().refv_last_error().decode())
 
     def info():
         out = np.zeros(2, np.int64)

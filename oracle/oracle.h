@@ -7,14 +7,12 @@
 //     pinned: tests compare them against the reference scalar library compiled
 //     from its own sources (oracle/_ref) and against tests/golden/ fixtures it
 //     wrote.
-//   * CSR5 and VHCC SpMV exist in the reference only as RVV intrinsics
-//     (src/rvv/).  Those files compile unmodified against the scalar
-//     intrinsic stand-in rvv_emul/riscv_vector.h (oracle/_ref/libref_rvv.so),
-//     and tests run them on this oracle's layouts: both are pinned.
-//   * VNEC (S/D/L) SpMV is restated from src/rvv/spmv_mtx_vnec.cpp, whose
-//     kernels read structures no reference code fills; it is pinned only
-//     indirectly, against the long-double CSR result on the same matrix
-//     ("parity unpinned" by the reference itself).
+//   * CSR5, VHCC and VNEC (D/S/L) SpMV exist in the reference only as RVV
+//     intrinsics (src/rvv/).  Those files compile unmodified against the
+//     scalar intrinsic stand-in rvv_emul/riscv_vector.h
+//     (oracle/_ref/libref_rvv.so), and tests run them on this oracle's
+//     layouts (for VNEC the shim also sets the structures its kernels read,
+//     which no reference code fills): all three are pinned.
 //   * The reference ships no builder for SELL-C-sigma, CSR5, LAV, VNEC S/D,
 //     VHCC or CVR.  The builders here define the layout each reference kernel
 //     reads; they are pinned by round trips (format -> CSR == source) and by

@@ -18,8 +18,11 @@
 #include "riscv_vector.h"
 #include "sparse_matrix.h"
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <exception>
 #include <string>
 #include <vector>
@@ -169,12 +172,17 @@ REFV_VHCC(float, f32)
 // ---------------------------------------------------------------- VNEC
 // info[0..1] = vnec_t (0 D, 1 S, 2 L), NUM_THREADS_VNEC; *ird = IRD_mat
 #define REFV_VNEC(VT, S)                                                                      \
+  /* threads > 0: the OpenMP team size while the constructor runs (it sets    */           \
+  /* NUM_THREADS_VNEC from it and computes IRD with that many threads).       */           \
   void* refv_vnec_new_##S(int64_t m, int64_t n, int64_t nz, const int* Rst, const int* Col,   \
-                          const VT* Val) {                                                    \
+                          const VT* Val, int threads) {                                       \
     try {                                                                                     \
       auto* box = new VnecBox<VT>();                                                          \
       box->G = spMtxCRS<VT>((size_t)m, (size_t)n, (size_t)nz, Rst, Col, Val);                 \
+      const int saved = omp_get_max_threads();                                                \
+      if (threads > 0) omp_set_num_threads(threads);                                          \
       box->A = new spMtxVNEC<VT>(box->G);                                                     \
+      omp_set_num_threads(saved);                                                             \
       box->b.assign((size_t)n, VT(0));                                                        \
       box->y.assign((size_t)m, VT(0));                                                        \
       return box;                                                                             \
@@ -199,5 +207,77 @@ REFV_VHCC(float, f32)
   }
 REFV_VNEC(double, f64)
 REFV_VNEC(float, f32)
+
+// The reference's VNEC kernels read structures that no reference code fills
+// (the constructor computes only IRD and the variant): this sets them from a
+// layout the oracle's VNEC builder made for the same matrix, allocated the way
+// the reference's freeMem() releases them (include/VNEC.h:265-319: malloc'd
+// arrays, NUM_THREADS_VNEC + 1 slots for use_x_indices / ecr_xx_val, one
+// malloc'd row list per thread in tasks), then selects the variant.
+// ints[0..1] = vnec_t (0 D, 1 S, 2 L), NUM_THREADS_VNEC (<= 256, the D and L
+//              kernels' carry arrays)
+// lens[0..7] = |ecr_indices|, |use_x_indices|, |v_row_ptr|, |col_start|,
+//              |val_align|, |tasks|, |row_begin| (= |row_end|), |reorder_col|
+// Arrays a variant does not use may be NULL (their lengths 0).
+}  // extern "C"
+namespace {
+template <class T>
+T* dup(const T* src, int64_t n, int64_t pad = 0) {
+  T* p = (T*)std::calloc((size_t)(n + pad > 0 ? n + pad : 1), sizeof(T));
+  if (p && src && n > 0) std::memcpy(p, src, (size_t)n * sizeof(T));
+  return p;
+}
+}  // namespace
+extern "C" {
+#define REFV_VNEC_FILL(VT, S)                                                                 \
+  int refv_vnec_fill_##S(void* h, const int64_t* ints, const int64_t* lens, const int* tcs,    \
+                         const int* tce, const int* nec, const int* ux_ptr, const int* ux,     \
+                         const int* ecr, const int* vrp, const int* cs, const VT* va,          \
+                         const int* tasks, const int* ts, const int* te, const int* sv,        \
+                         const int* rb, const int* re, const int* rc, const VT* rv) {          \
+    auto& A = *((VnecBox<VT>*)h)->A;                                                          \
+    const int NT = (int)ints[1];                                                              \
+    if (NT < 1 || NT > 256 || ints[0] < 0 || ints[0] > 2) {                                   \
+      g_last_error = "refv_vnec_fill: bad variant or thread count";                            \
+      return -1;                                                                              \
+    }                                                                                         \
+    A.freeMem();                                                                              \
+    A.NUM_THREADS_VNEC = NT;                                                                  \
+    A.vnec_t = (SpB_VNEC_type)ints[0];                                                        \
+    A.thread_coord_start = (coord*)dup(tcs, 2 * (int64_t)NT);                                 \
+    A.thread_coord_end = (coord*)dup(tce, 2 * (int64_t)NT);                                   \
+    const int64_t nl = std::is_same<VT, float>::value ? nLanes_f32 : nLanes_f64;              \
+    if (nec) {                                                                                \
+      A.NEC_NUM = dup(nec, NT);                                                               \
+      A.use_x_indices = (int**)std::calloc((size_t)NT + 1, sizeof(int*));                     \
+      A.ecr_xx_val = (VT**)std::calloc((size_t)NT + 1, sizeof(VT*));                          \
+      for (int t = 0; t < NT; ++t) {                                                          \
+        A.use_x_indices[t] = dup(ux + ux_ptr[t], (int64_t)nec[t], nl);                        \
+        A.ecr_xx_val[t] = dup<VT>(nullptr, (int64_t)nec[t], nl);                              \
+      }                                                                                       \
+    }                                                                                         \
+    if (ecr) A.ecr_indices = dup(ecr, lens[0]);                                               \
+    if (vrp) A.v_row_ptr = dup(vrp, lens[2]);                                                 \
+    if (cs) A.col_start = dup(cs, lens[3]);                                                   \
+    if (va) A.val_align = dup(va, lens[4]);                                                   \
+    if (tasks) {                                                                              \
+      A.tasks = (int**)std::calloc((size_t)NT, sizeof(int*));                                 \
+      for (int t = 0; t < NT; ++t) {                                                          \
+        const int64_t cnt = std::max<int64_t>((int64_t)te[t] - ts[t], (int64_t)sv[t]);        \
+        const int64_t avail = std::max<int64_t>(0, std::min<int64_t>(cnt, lens[5] - ts[t]));  \
+        A.tasks[t] = dup(tasks + ts[t], avail, cnt - avail + nl);                             \
+      }                                                                                       \
+      A.spvv_len = dup(sv, NT);                                                               \
+      A.reorder_mat.task_start = dup(ts, NT);                                                 \
+      A.reorder_mat.task_end = dup(te, NT);                                                   \
+      A.reorder_mat.row_begin = dup(rb, lens[6], nl);                                         \
+      A.reorder_mat.row_end = dup(re, lens[6], nl);                                           \
+      A.reorder_mat.col = dup(rc, lens[7], nl);                                               \
+      A.reorder_mat.nnz = dup(rv, lens[7], nl);                                               \
+    }                                                                                         \
+    return 0;                                                                                 \
+  }
+REFV_VNEC_FILL(double, f64)
+REFV_VNEC_FILL(float, f32)
 
 }  // extern "C"

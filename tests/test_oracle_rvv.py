@@ -1,14 +1,17 @@
-"""Pinning the oracle's CSR5 and VHCC restatements to the reference's own
-RVV-only kernels (src/rvv/spmv_mtx_csr5.cpp, src/rvv/spmv_vhcc.cpp), compiled
-unmodified for x86-64 against the scalar intrinsic stand-in
-oracle/rvv_emul/riscv_vector.h (VLEN 256) into oracle/_ref/libref_rvv.so.
+"""Pinning the oracle's CSR5, VHCC and VNEC restatements to the reference's
+own RVV-only kernels (src/rvv/spmv_mtx_csr5.cpp, src/rvv/spmv_vhcc.cpp,
+src/rvv/spmv_mtx_vnec.cpp), compiled unmodified for x86-64 against the
+scalar intrinsic stand-in oracle/rvv_emul/riscv_vector.h (VLEN 256) into
+oracle/_ref/libref_rvv.so.
 
-The reference has no builder for either format, so both sides run on the
-same layout from the oracle's builders; the reference computes with its own
-vector code (fused multiply-adds, its reductions, its thread split), so the
-check is normwise, at the restatement tolerances (1e-12 fp64, 1e-5 fp32),
-against the restatement and against the long-double CSR oracle.  Also
-pinned here: the stand-in's own semantics on small known cases."""
+The reference has no builder for CSR5 or VHCC and fills none of VNEC's
+kernel structures, so both sides run on the same layout from the oracle's
+builders; the reference computes with its own vector code (fused
+multiply-adds, its reductions, its thread split), so the check is normwise,
+at the restatement tolerances (1e-12 fp64, 1e-5 fp32), against the
+restatement and against the long-double CSR oracle.  The reference defects
+met on the way are pinned as such (CSR5 sigma > omega, VNEC-D rows spanning
+threads)."""
 import numpy as np
 import pytest
 
@@ -122,3 +125,75 @@ def test_vhcc_reference_rejects_other_vector_sizes():
     m, n, R, C, V = W.powerlaw(500, seed=2)
     with pytest.raises(ValueError):
         O.refv_vhcc(O.build_vhcc(O.crs(m, n, R, C, V), 2, 32))
+
+
+# ------------------------------------------------------------------ VNEC
+def inside_one_row(b, Rst):
+    """Some thread's range starts inside a row and ends in the same row."""
+    tcs = np.asarray(b["thread_coord_start"]).reshape(-1, 2)
+    tce = np.asarray(b["thread_coord_end"]).reshape(-1, 2)
+    return any(s[0] == e[0] and s[1] > Rst[s[0]] for s, e in zip(tcs, tce))
+
+
+def test_vnec_d_reference_double_counts_rows_spanning_threads():
+    """The reference's VNEC-D carry for a thread that starts and ends inside
+    one row sums that row from the row's own start (src/rvv/
+    spmv_mtx_vnec.cpp:364-446), counting the previous threads' share again;
+    the restatement and the GPU kernel start at max(row start, thread
+    start).  One 10,000-entry row split over 4 threads shows it."""
+    g = load_golden([p for p in GOLD if "one_long_row_f64" in p][0])
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    b = O.build_vnec(src, 4, 0)
+    assert inside_one_row(b, g["Rst"])
+    yld = O.crs_spmv_ld(src, g["alpha"], g["x"], g["beta"], g["y0"])
+    assert O.normwise_relerr(O.spmv(b, g["alpha"], g["x"], g["beta"], g["y0"]), yld) < 1e-12
+    assert O.normwise_relerr(O.refv_vnec(src, b).spmv(g["alpha"], g["x"], g["beta"], g["y0"]), yld) > 1e-3
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_vnec_reference_kernels_golden(g, variant):
+    """D (0), S (1) and L (2): the reference's kernels (src/rvv/
+    spmv_mtx_vnec.cpp:192-586) run on the structures of the oracle's builder,
+    which the reference itself never fills."""
+    dt = g["Val"].dtype
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    for threads in (1, 4):
+        b = O.build_vnec(src, threads, variant)
+        ref = O.refv_vnec(src, b)
+        assert ref.info()["vnec_t"] == variant and ref.info()["threads"] == threads
+        if variant in (0, 2) and inside_one_row(b, g["Rst"]):
+            # D: the reference's carry bug, pinned separately below; L: its
+            # carry fix-up adds the carries of threads that end in the same
+            # row concurrently (src/rvv/spmv_mtx_vnec.cpp:580-585), a race
+            continue
+        for alpha, beta in ((g["alpha"], g["beta"]), (1.0, 0.0)):
+            yr = ref.spmv(alpha, g["x"], beta, g["y0"])
+            assert O.normwise_relerr(yr, O.spmv(b, alpha, g["x"], beta, g["y0"])) < tol_for(dt)
+            assert O.normwise_relerr(yr, O.crs_spmv_ld(src, alpha, g["x"], beta, g["y0"])) < tol_for(dt)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_vnec_reference_kernels_powerlaw(dt):
+    m, n, R, C, V = W.powerlaw(3000, seed=3)
+    src = O.crs(m, n, R, C, V.astype(dt))
+    x, y0 = W.vector(n, 0).astype(dt), W.vector(m, 1).astype(dt)
+    for variant in (0, 1, 2):
+        for threads in (1, 8):
+            b = O.build_vnec(src, threads, variant)
+            yr = O.refv_vnec(src, b).spmv(1.25, x, 0.5, y0)
+            assert O.normwise_relerr(yr, O.spmv(b, 1.25, x, 0.5, y0)) < tol_for(dt), (variant, threads)
+            assert O.normwise_relerr(yr, O.crs_spmv_ld(src, 1.25, x, 0.5, y0)) < tol_for(dt), (variant, threads)
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_vnec_ird_and_variant_match_reference_single_thread(dt):
+    """The reference constructor's IRD and D/S choice (include/VNEC.h:78-227)
+    on one OpenMP thread; with more threads its IRD_VNEC races on a shared
+    group counter, so only the one-thread value is a fixed point."""
+    for m, n, R, C, V in (W.powerlaw(3000, seed=3), W.powerlaw(2500, band=8, seed=9)):
+        src = O.crs(m, n, R, C, V.astype(dt))
+        info = O.refv_vnec(src, threads=1).info()
+        ours = O.build_vnec(src, 1, -1)
+        assert info["threads"] == 1
+        assert abs(info["IRD_mat"] - float(ours["IRD_mat"])) <= 1e-6 * max(1.0, abs(info["IRD_mat"]))
+        assert info["vnec_t"] == int(ours["vnec_t"])
