@@ -8,10 +8,11 @@ Two libraries, both built by ``oracle/Makefile``:
   (RVVLASparse src/scalar/*.cpp) compiled where they lie, behind the
   ``extern "C"`` shim ref_shim.cpp.  Built only where the reference sources
   are present; the built file travels with the repository snapshot.
-* ``_ref/libref_rvv.so`` — the reference's RVV-only kernels (CSR5, VNEC,
-  VHCC: src/rvv/spmv_mtx_csr5.cpp, spmv_mtx_vnec.cpp, spmv_vhcc.cpp) compiled
-  where they lie against the scalar intrinsic stand-in
-  ``rvv_emul/riscv_vector.h`` (VLEN 256), behind the shim rvv_shim.cpp.
+* ``_ref/libref_rvv.so`` — the reference's RVV sources (src/rvv/*.cpp: the
+  CSR5, VNEC and VHCC kernels, which exist only there, and the RVV CRS, HCSR,
+  SELL and LAV products) compiled where they lie against the scalar intrinsic
+  stand-in ``rvv_emul/riscv_vector.h`` (VLEN 256), behind the shims
+  rvv_shim.cpp (names refv_*) and ref_shim.cpp built for simd = true (refr_*).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` may import this package, and only as the checker / the timed CPU
@@ -274,18 +275,28 @@ def ref_available() -> bool:
     return os.path.exists(REF_LIB)
 
 
-def _ref():
+def _ref(simd: bool = False):
+    """The reference library: its scalar specialisations sparse_mv<T, Fmt,
+    false> (libref_scalar.so, names refx_*) or, with ``simd``, its RVV ones
+    sparse_mv<T, Fmt, true> on the intrinsic stand-in (libref_rvv.so, names
+    refr_*; CRS, HCSR, SELL, LAV — the reference has no RVV CVR)."""
     global _rlib
     if _rlib is None:
-        if not os.path.exists(REF_LIB):
-            raise RuntimeError("reference scalar library not built (make -C oracle ref)")
-        L = C.CDLL(REF_LIB)
+        _rlib = {}
+    if simd not in _rlib:
+        path, pre = (REFV_LIB, "refr_") if simd else (REF_LIB, "refx_")
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference library {os.path.basename(path)} not built (make -C oracle ref)")
+        L = C.CDLL(path)
         vp, i64, dbl, flt, cint = C.c_void_p, C.c_int64, C.c_double, C.c_float, C.c_int
-        L.refx_last_error.restype = C.c_char_p
-        L.refx_num_threads.restype = cint
+        getattr(L, pre + "last_error").restype = C.c_char_p
+        getattr(L, pre + "num_threads").restype = cint
         for S, T in (("f64", dbl), ("f32", flt)):
             def p(name, res, args):
-                f = getattr(L, name.replace("@", S))
+                name = name.replace("refx_", pre).replace("@", S)
+                if not hasattr(L, name):  # CVR in the RVV library
+                    return
+                f = getattr(L, name)
                 f.restype, f.argtypes = res, args
             p("refx_crs_new_@", vp, [i64, i64, i64, vp, vp, vp])
             p("refx_crs_free_@", None, [vp])
@@ -310,8 +321,9 @@ def _ref():
             p("refx_cvr_free_@", None, [vp])
             p("refx_cvr_spmv_@", cint, [vp, T, vp, T, vp])
             p("refx_cvr_time_@", dbl, [vp, T, vp, T, cint])
-        _rlib = L
-    return _rlib
+        L.prefix = pre
+        _rlib[simd] = L
+    return _rlib[simd]
 
 
 def _sfx(dt) -> str:
@@ -323,43 +335,44 @@ def _a(x, dt):
 
 
 class RefMatrix:
-    """A matrix held by the reference library (owning handle)."""
+    """A matrix held by the reference library (owning handle); ``simd``
+    selects its RVV specialisations."""
 
-    def __init__(self, kind: str, handle, dt, keep=()):
-        self.kind, self.h, self.dt, self._keep = kind, handle, np.dtype(dt), keep
+    def __init__(self, kind: str, handle, dt, keep=(), simd: bool = False):
+        self.kind, self.h, self.dt, self._keep, self.simd = kind, handle, np.dtype(dt), keep, simd
+
+    def _fn(self, what: str):
+        L = _ref(self.simd)
+        return getattr(L, f"{L.prefix}{self.kind}_{what}_{_sfx(self.dt)}")
 
     def __del__(self):
         try:
-            getattr(_ref(), f"refx_{self.kind}_free_{_sfx(self.dt)}")(self.h)
+            self._fn("free")(self.h)
         except Exception:
             pass
 
     def spmv(self, alpha, b, beta, y, stage: int | None = None) -> np.ndarray:
-        L = _ref()
         b = _a(b, self.dt)
         out = np.array(y, dtype=self.dt, copy=True)
         if self.kind == "sell":
-            rc = getattr(L, f"refx_sell_spmv_{_sfx(self.dt)}")(self.h, 3 if stage is None else stage, alpha,
-                                                               b.ctypes.data, beta, out.ctypes.data)
+            rc = self._fn("spmv")(self.h, 3 if stage is None else stage, alpha, b.ctypes.data, beta, out.ctypes.data)
         else:
-            rc = getattr(L, f"refx_{self.kind}_spmv_{_sfx(self.dt)}")(self.h, alpha, b.ctypes.data, beta,
-                                                                     out.ctypes.data)
+            rc = self._fn("spmv")(self.h, alpha, b.ctypes.data, beta, out.ctypes.data)
         assert rc == 0
         return out
 
     def time(self, alpha, b, beta, iters: int) -> float:
-        L = _ref()
         b = _a(b, self.dt)
-        return getattr(L, f"refx_{self.kind}_time_{_sfx(self.dt)}")(self.h, alpha, b.ctypes.data, beta, iters)
+        return self._fn("time")(self.h, alpha, b.ctypes.data, beta, iters)
 
 
-def ref_crs(src: Bundle) -> RefMatrix:
+def ref_crs(src: Bundle, simd: bool = False) -> RefMatrix:
     dt = src.dtype
-    L = _ref()
+    L = _ref(simd)
     Rst, Col, Val = _a(src["Rst"], np.int32), _a(src["Col"], np.int32), _a(src["Val"], dt)
-    h = getattr(L, f"refx_crs_new_{_sfx(dt)}")(int(src["m"]), int(src["n"]), int(src["nz"]), Rst.ctypes.data,
+    h = getattr(L, f"{L.prefix}crs_new_{_sfx(dt)}")(int(src["m"]), int(src["n"]), int(src["nz"]), Rst.ctypes.data,
                                                 Col.ctypes.data, Val.ctypes.data)
-    return RefMatrix("crs", h, dt)
+    return RefMatrix("crs", h, dt, simd=simd)
 
 
 def ref_hcsr_convert(src: Bundle, R=None, C_=None, p=None) -> Bundle:
@@ -386,30 +399,30 @@ def ref_hcsr_convert(src: Bundle, R=None, C_=None, p=None) -> Bundle:
     return Bundle("hcsr", arrs, sc)
 
 
-def ref_hcsr(b: Bundle) -> RefMatrix:
-    L = _ref()
+def ref_hcsr(b: Bundle, simd: bool = False) -> RefMatrix:
+    L = _ref(simd)
     dt = b.dtype
     info = np.array([b[k] for k in ("R", "C", "m", "n", "nz", "b_m", "b_n")], np.int64)
     arrs = [_a(b["block_ptr"], np.int32), _a(b["row_offset"], np.uint32), _a(b["row_ptr"], np.uint32),
             _a(b["col_idx"], np.uint16), _a(b["values"], dt)]
     sizes = np.array([len(a) for a in arrs], np.int64)
-    h = getattr(L, f"refx_hcsr_new_{_sfx(dt)}")(info.ctypes.data, *(a.ctypes.data for a in arrs), sizes.ctypes.data)
-    return RefMatrix("hcsr", h, dt)
+    h = getattr(L, f"{L.prefix}hcsr_new_{_sfx(dt)}")(info.ctypes.data, *(a.ctypes.data for a in arrs), sizes.ctypes.data)
+    return RefMatrix("hcsr", h, dt, simd=simd)
 
 
-def ref_sell(b: Bundle) -> RefMatrix:
-    L = _ref()
+def ref_sell(b: Bundle, simd: bool = False) -> RefMatrix:
+    L = _ref(simd)
     dt = b.dtype
     ints = np.array([b[k] for k in ("m", "n", "cnt_b", "nz", "C", "Sigma")], np.int64)
     arrs = [_a(b[k], np.int32) for k in ("vCl", "vCs", "vBs", "vSBs")]
     col, perm, val = _a(b["vCol"], np.uint32), _a(b["vPerm"], np.uint32), _a(b["vVal"], dt)
-    h = getattr(L, f"refx_sell_new_{_sfx(dt)}")(ints.ctypes.data, *(a.ctypes.data for a in arrs), col.ctypes.data,
+    h = getattr(L, f"{L.prefix}sell_new_{_sfx(dt)}")(ints.ctypes.data, *(a.ctypes.data for a in arrs), col.ctypes.data,
                                                 perm.ctypes.data, val.ctypes.data, len(col))
-    return RefMatrix("sell", h, dt, keep=(arrs, col, perm, val))
+    return RefMatrix("sell", h, dt, keep=(arrs, col, perm, val), simd=simd)
 
 
-def ref_lav(b: Bundle) -> RefMatrix:
-    L = _ref()
+def ref_lav(b: Bundle, simd: bool = False) -> RefMatrix:
+    L = _ref(simd)
     dt = b.dtype
     ints = np.array([b[k] for k in ("SIMD_Lanes", "m", "n", "nz", "segment_count", "chunk_count", "segment_len")]
                     + [0], np.int64)
@@ -418,11 +431,11 @@ def ref_lav(b: Bundle) -> RefMatrix:
     val, ci = _a(b["val"], dt), _a(b["col_id"], np.uint32)
     sR, sC, sV = _a(b["sp_Rst"], np.int32), _a(b["sp_Col"], np.int32), _a(b["sp_Val"], dt)
     lens = np.array([len(co), len(cf), len(sp), len(oo), len(mk), len(val), len(sC)], np.int64)
-    h = getattr(L, f"refx_lav_new_{_sfx(dt)}")(ints.ctypes.data, float(b["T"]), lens.ctypes.data, co.ctypes.data,
+    h = getattr(L, f"{L.prefix}lav_new_{_sfx(dt)}")(ints.ctypes.data, float(b["T"]), lens.ctypes.data, co.ctypes.data,
                                                cf.ctypes.data, sp.ctypes.data, oo.ctypes.data, mk.ctypes.data,
                                                val.ctypes.data, ci.ctypes.data, sR.ctypes.data, sC.ctypes.data,
                                                sV.ctypes.data)
-    return RefMatrix("lav", h, dt)
+    return RefMatrix("lav", h, dt, simd=simd)
 
 
 def ref_cvr(b: Bundle) -> RefMatrix:

@@ -26,6 +26,21 @@
 
 using namespace SparseMatrixLib;
 
+// Built twice by oracle/Makefile: into libref_scalar.so with the defaults
+// (the reference's scalar specialisations sparse_mv<T, Fmt, false>, names
+// refx_*) and into libref_rvv.so with -DREFX_SIMD=true -DREFX_PREFIX=refr_
+// (its RVV specialisations sparse_mv<T, Fmt, true> from src/rvv/, on the
+// scalar intrinsic stand-in, names refr_*).  Builders stay the scalar ones.
+#ifndef REFX_SIMD
+#define REFX_SIMD false
+#endif
+#ifndef REFX_PREFIX
+#define REFX_PREFIX refx_
+#endif
+#define REFX_CAT2(a, b) a##b
+#define REFX_CAT(a, b) REFX_CAT2(a, b)
+#define REFX_FN(name) REFX_CAT(REFX_PREFIX, name)
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -71,31 +86,31 @@ double time_loop(Box* box, int iters, Fn&& fn) {
 
 extern "C" {
 
-const char* refx_last_error() { return g_last_error.c_str(); }
-int refx_num_threads() { return omp_get_max_threads(); }
+const char* REFX_FN(last_error)() { return g_last_error.c_str(); }
+int REFX_FN(num_threads)() { return omp_get_max_threads(); }
 
 // ---------------------------------------------------------------- CRS
 #define REFX_CRS(VT, S)                                                                       \
-  void* refx_crs_new_##S(int64_t m, int64_t n, int64_t nz, const int* Rst, const int* Col,   \
+  void* REFX_FN(crs_new_##S)(int64_t m, int64_t n, int64_t nz, const int* Rst, const int* Col,   \
                          const VT* Val) {                                                     \
     return crs_new<VT>(m, n, nz, Rst, Col, Val);                                              \
   }                                                                                          \
-  void refx_crs_free_##S(void* h) { delete (CrsBox<VT>*)h; }                                  \
-  int refx_crs_spmv_##S(void* h, VT alpha, const VT* b, VT beta, VT* y) {                        \
+  void REFX_FN(crs_free_##S)(void* h) { delete (CrsBox<VT>*)h; }                                  \
+  int REFX_FN(crs_spmv_##S)(void* h, VT alpha, const VT* b, VT beta, VT* y) {                        \
     auto* box = (CrsBox<VT>*)h;                                                               \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     std::memcpy(box->y.data(), y, box->y.size() * sizeof(VT));                                \
-    sparse_matrix_status st = sparse_mv<VT, spMtxCRS, false>(                                 \
+    sparse_matrix_status st = sparse_mv<VT, spMtxCRS, REFX_SIMD>(                                 \
         SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A, sparse_matrix_descr{}, box->b, beta,  \
         box->y);                                                                             \
     std::memcpy(y, box->y.data(), box->y.size() * sizeof(VT));                                \
     return st.code;                                                                          \
   }                                                                                          \
-  double refx_crs_time_##S(void* h, VT alpha, const VT* b, VT beta, int iters) {                \
+  double REFX_FN(crs_time_##S)(void* h, VT alpha, const VT* b, VT beta, int iters) {                \
     auto* box = (CrsBox<VT>*)h;                                                               \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     return time_loop(box, iters, [&] {                                                       \
-      sparse_mv<VT, spMtxCRS, false>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,           \
+      sparse_mv<VT, spMtxCRS, REFX_SIMD>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,           \
                                     sparse_matrix_descr{}, box->b, beta, box->y);            \
     });                                                                                      \
   }
@@ -106,7 +121,7 @@ REFX_CRS(float, f32)
 // info[0..6] = R, C, m, n, nz, b_m, b_n ; sizes[0..4] = |block_ptr|, |row_offset|,
 // |row_ptr|, |col_idx|, |values|
 #define REFX_HCSR(VT, S)                                                                      \
-  void* refx_hcsr_convert_##S(void* crs, int R, int C, double p, int set_R, int set_C,       \
+  void* REFX_FN(hcsr_convert_##S)(void* crs, int R, int C, double p, int set_R, int set_C,       \
                               int set_p) {                                                   \
     auto* src = (CrsBox<VT>*)crs;                                                             \
     auto* box = new FmtBox<spMtxHCSR<VT>, VT>();                                               \
@@ -125,7 +140,7 @@ REFX_CRS(float, f32)
     box->y.assign(box->A.m, VT(0));                                                           \
     return box;                                                                              \
   }                                                                                          \
-  void* refx_hcsr_new_##S(const int64_t* info, const int* block_ptr,                         \
+  void* REFX_FN(hcsr_new_##S)(const int64_t* info, const int* block_ptr,                         \
                           const uint32_t* row_offset, const uint32_t* row_ptr,               \
                           const uint16_t* col_idx, const VT* values, const int64_t* sizes) {  \
     auto* box = new FmtBox<spMtxHCSR<VT>, VT>();                                               \
@@ -142,8 +157,8 @@ REFX_CRS(float, f32)
     box->y.assign(A.m, VT(0));                                                                \
     return box;                                                                              \
   }                                                                                          \
-  void refx_hcsr_free_##S(void* h) { delete (FmtBox<spMtxHCSR<VT>, VT>*)h; }                   \
-  void refx_hcsr_info_##S(void* h, int64_t* info, int64_t* sizes) {                          \
+  void REFX_FN(hcsr_free_##S)(void* h) { delete (FmtBox<spMtxHCSR<VT>, VT>*)h; }                   \
+  void REFX_FN(hcsr_info_##S)(void* h, int64_t* info, int64_t* sizes) {                          \
     auto& A = ((FmtBox<spMtxHCSR<VT>, VT>*)h)->A;                                              \
     info[0] = (int64_t)A.R; info[1] = (int64_t)A.C; info[2] = (int64_t)A.m;                  \
     info[3] = (int64_t)A.n; info[4] = (int64_t)A.nz; info[5] = (int64_t)A.b_m;               \
@@ -152,7 +167,7 @@ REFX_CRS(float, f32)
     sizes[2] = (int64_t)A.row_ptr.size(); sizes[3] = (int64_t)A.col_idx.size();              \
     sizes[4] = (int64_t)A.values.size();                                                     \
   }                                                                                          \
-  void refx_hcsr_export_##S(void* h, int* block_ptr, uint32_t* row_offset,                   \
+  void REFX_FN(hcsr_export_##S)(void* h, int* block_ptr, uint32_t* row_offset,                   \
                             uint32_t* row_ptr, uint16_t* col_idx, VT* values) {               \
     auto& A = ((FmtBox<spMtxHCSR<VT>, VT>*)h)->A;                                              \
     std::memcpy(block_ptr, A.block_ptr.data(), A.block_ptr.size() * sizeof(int));            \
@@ -161,21 +176,21 @@ REFX_CRS(float, f32)
     std::memcpy(col_idx, A.col_idx.data(), A.col_idx.size() * sizeof(uint16_t));             \
     std::memcpy(values, A.values.data(), A.values.size() * sizeof(VT));                       \
   }                                                                                          \
-  int refx_hcsr_spmv_##S(void* h, VT alpha, const VT* b, VT beta, VT* y) {                       \
+  int REFX_FN(hcsr_spmv_##S)(void* h, VT alpha, const VT* b, VT beta, VT* y) {                       \
     auto* box = (FmtBox<spMtxHCSR<VT>, VT>*)h;                                                 \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     std::memcpy(box->y.data(), y, box->y.size() * sizeof(VT));                                \
-    sparse_matrix_status st = sparse_mv<VT, spMtxHCSR, false>(                                \
+    sparse_matrix_status st = sparse_mv<VT, spMtxHCSR, REFX_SIMD>(                                \
         SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A, sparse_matrix_descr{}, box->b, beta,  \
         box->y);                                                                             \
     std::memcpy(y, box->y.data(), box->y.size() * sizeof(VT));                                \
     return st.code;                                                                          \
   }                                                                                          \
-  double refx_hcsr_time_##S(void* h, VT alpha, const VT* b, VT beta, int iters) {               \
+  double REFX_FN(hcsr_time_##S)(void* h, VT alpha, const VT* b, VT beta, int iters) {               \
     auto* box = (FmtBox<spMtxHCSR<VT>, VT>*)h;                                                 \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     return time_loop(box, iters, [&] {                                                       \
-      sparse_mv<VT, spMtxHCSR, false>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,          \
+      sparse_mv<VT, spMtxHCSR, REFX_SIMD>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,          \
                                      sparse_matrix_descr{}, box->b, beta, box->y);           \
     });                                                                                      \
   }
@@ -185,7 +200,7 @@ REFX_HCSR(float, f32)
 // ---------------------------------------------------------------- SELL-C-sigma
 // ints[0..5] = m, n, cnt_b, nz, C, Sigma ; len = |vCol| = |vVal|
 #define REFX_SELL(VT, S)                                                                      \
-  void* refx_sell_new_##S(const int64_t* ints, const int* vCl, const int* vCs, const int* vBs, \
+  void* REFX_FN(sell_new_##S)(const int64_t* ints, const int* vCl, const int* vCs, const int* vBs, \
                           const int* vSBs, const uint32_t* vCol, const uint32_t* vPerm,      \
                           const VT* vVal, int64_t len) {                                      \
     auto* box = new FmtBox<spMtxSELL_C_Sigma<VT>, VT>();                                       \
@@ -200,8 +215,8 @@ REFX_HCSR(float, f32)
     box->y.assign(A.m, VT(0));                                                                \
     return box;                                                                              \
   }                                                                                          \
-  void refx_sell_free_##S(void* h) { delete (FmtBox<spMtxSELL_C_Sigma<VT>, VT>*)h; }           \
-  int refx_sell_spmv_##S(void* h, int stage, VT alpha, const VT* b, VT beta, VT* y) {            \
+  void REFX_FN(sell_free_##S)(void* h) { delete (FmtBox<spMtxSELL_C_Sigma<VT>, VT>*)h; }           \
+  int REFX_FN(sell_spmv_##S)(void* h, int stage, VT alpha, const VT* b, VT beta, VT* y) {            \
     auto* box = (FmtBox<spMtxSELL_C_Sigma<VT>, VT>*)h;                                         \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     std::memcpy(box->y.data(), y, box->y.size() * sizeof(VT));                                \
@@ -209,23 +224,23 @@ REFX_HCSR(float, f32)
     auto op = SPARSE_OPERATION_NON_TRANSPOSE;                                                \
     auto d = sparse_matrix_descr{};                                                          \
     switch (stage) {                                                                         \
-      case 0: st = sparse_mv<VT, spMtxSELL_C_Sigma, false, SPARSE_MATRIX_MV_PREPARATION>(     \
+      case 0: st = sparse_mv<VT, spMtxSELL_C_Sigma, REFX_SIMD, SPARSE_MATRIX_MV_PREPARATION>(     \
                   op, alpha, box->A, d, box->b, beta, box->y); break;                        \
-      case 1: st = sparse_mv<VT, spMtxSELL_C_Sigma, false, SPARSE_MATRIX_MV_MULT>(            \
+      case 1: st = sparse_mv<VT, spMtxSELL_C_Sigma, REFX_SIMD, SPARSE_MATRIX_MV_MULT>(            \
                   op, alpha, box->A, d, box->b, beta, box->y); break;                        \
-      case 2: st = sparse_mv<VT, spMtxSELL_C_Sigma, false, SPARSE_MATRIX_MV_GET_RESULTS>(     \
+      case 2: st = sparse_mv<VT, spMtxSELL_C_Sigma, REFX_SIMD, SPARSE_MATRIX_MV_GET_RESULTS>(     \
                   op, alpha, box->A, d, box->b, beta, box->y); break;                        \
-      default: st = sparse_mv<VT, spMtxSELL_C_Sigma, false, SPARSE_MATRIX_MV_ALL_STAGES>(     \
+      default: st = sparse_mv<VT, spMtxSELL_C_Sigma, REFX_SIMD, SPARSE_MATRIX_MV_ALL_STAGES>(     \
                   op, alpha, box->A, d, box->b, beta, box->y); break;                        \
     }                                                                                        \
     std::memcpy(y, box->y.data(), box->y.size() * sizeof(VT));                                \
     return st.code;                                                                          \
   }                                                                                          \
-  double refx_sell_time_##S(void* h, VT alpha, const VT* b, VT beta, int iters) {               \
+  double REFX_FN(sell_time_##S)(void* h, VT alpha, const VT* b, VT beta, int iters) {               \
     auto* box = (FmtBox<spMtxSELL_C_Sigma<VT>, VT>*)h;                                         \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     return time_loop(box, iters, [&] {                                                       \
-      sparse_mv<VT, spMtxSELL_C_Sigma, false, SPARSE_MATRIX_MV_ALL_STAGES>(                   \
+      sparse_mv<VT, spMtxSELL_C_Sigma, REFX_SIMD, SPARSE_MATRIX_MV_ALL_STAGES>(                   \
           SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A, sparse_matrix_descr{}, box->b,      \
           beta, box->y);                                                                     \
     });                                                                                      \
@@ -238,7 +253,7 @@ REFX_SELL(float, f32)
 // lens[0..6] = |chunk_offsets|, |chunk_offsets_full_mask|, |segment_ptr|, |out_order|,
 //              |mask|, |val| (= |col_id|), sparse nz
 #define REFX_LAV(VT, S)                                                                       \
-  void* refx_lav_new_##S(const int64_t* ints, double Tthr, const int64_t* lens,              \
+  void* REFX_FN(lav_new_##S)(const int64_t* ints, double Tthr, const int64_t* lens,              \
                          const int* chunk_offsets, const int* chunk_offsets_full_mask,       \
                          const uint64_t* segment_ptr, const uint32_t* out_order,             \
                          const uint16_t* mask, const VT* val, const uint32_t* col_id,         \
@@ -262,33 +277,37 @@ REFX_SELL(float, f32)
     box->y.assign((size_t)A.m, VT(0));                                                        \
     return box;                                                                              \
   }                                                                                          \
-  void refx_lav_free_##S(void* h) { delete (FmtBox<spMtxLAV<VT>, VT>*)h; }                     \
-  int refx_lav_spmv_##S(void* h, VT alpha, const VT* b, VT beta, VT* y) {                        \
+  void REFX_FN(lav_free_##S)(void* h) { delete (FmtBox<spMtxLAV<VT>, VT>*)h; }                     \
+  int REFX_FN(lav_spmv_##S)(void* h, VT alpha, const VT* b, VT beta, VT* y) {                        \
     auto* box = (FmtBox<spMtxLAV<VT>, VT>*)h;                                                  \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     std::memcpy(box->y.data(), y, box->y.size() * sizeof(VT));                                \
-    sparse_matrix_status st = sparse_mv<VT, spMtxLAV, false>(                                 \
+    sparse_matrix_status st = sparse_mv<VT, spMtxLAV, REFX_SIMD>(                                 \
         SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A, sparse_matrix_descr{}, box->b, beta,  \
         box->y);                                                                             \
     std::memcpy(y, box->y.data(), box->y.size() * sizeof(VT));                                \
     return st.code;                                                                          \
   }                                                                                          \
-  double refx_lav_time_##S(void* h, VT alpha, const VT* b, VT beta, int iters) {                \
+  double REFX_FN(lav_time_##S)(void* h, VT alpha, const VT* b, VT beta, int iters) {                \
     auto* box = (FmtBox<spMtxLAV<VT>, VT>*)h;                                                  \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     return time_loop(box, iters, [&] {                                                       \
-      sparse_mv<VT, spMtxLAV, false>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,           \
+      sparse_mv<VT, spMtxLAV, REFX_SIMD>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,           \
                                     sparse_matrix_descr{}, box->b, beta, box->y);            \
     });                                                                                      \
   }
 REFX_LAV(double, f64)
 REFX_LAV(float, f32)
 
+// src/rvv/spmv_mtx_cvr.cpp of the reference holds the scalar product again
+// (sparse_mv<T, spMtxCVR, false> only, :22 and :72): there is no simd = true
+// CVR, so the RVV build of this shim (-DREFX_SKIP_CVR=1) leaves CVR out.
+#if !defined(REFX_SKIP_CVR) || !REFX_SKIP_CVR
 // ---------------------------------------------------------------- CVR
 // ints[0..5] = nItems, numRows, numCols, SIMD_LEN, Nthreads, Nthreads_avail
 // lens[0..2] = |vPack_vec_vals| (= |cols|), |vPack_vec_record|, |writeback_pos_record|
 #define REFX_CVR(VT, S)                                                                       \
-  void* refx_cvr_new_##S(const int64_t* ints, const int64_t* lens, const VT* vals,            \
+  void* REFX_FN(cvr_new_##S)(const int64_t* ints, const int64_t* lens, const VT* vals,            \
                          const uint32_t* cols, const int* record, const int* writeback) {    \
     auto* box = new FmtBox<spMtxCVR<VT>, VT>();                                                \
     auto& A = box->A;                                                                        \
@@ -302,26 +321,27 @@ REFX_LAV(float, f32)
     box->y.assign(A.numRows, VT(0));                                                          \
     return box;                                                                              \
   }                                                                                          \
-  void refx_cvr_free_##S(void* h) { delete (FmtBox<spMtxCVR<VT>, VT>*)h; }                     \
-  int refx_cvr_spmv_##S(void* h, VT alpha, const VT* b, VT beta, VT* y) {                        \
+  void REFX_FN(cvr_free_##S)(void* h) { delete (FmtBox<spMtxCVR<VT>, VT>*)h; }                     \
+  int REFX_FN(cvr_spmv_##S)(void* h, VT alpha, const VT* b, VT beta, VT* y) {                        \
     auto* box = (FmtBox<spMtxCVR<VT>, VT>*)h;                                                  \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     std::memcpy(box->y.data(), y, box->y.size() * sizeof(VT));                                \
-    sparse_matrix_status st = sparse_mv<VT, spMtxCVR, false>(                                 \
+    sparse_matrix_status st = sparse_mv<VT, spMtxCVR, REFX_SIMD>(                                 \
         SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A, sparse_matrix_descr{}, box->b, beta,  \
         box->y);                                                                             \
     std::memcpy(y, box->y.data(), box->y.size() * sizeof(VT));                                \
     return st.code;                                                                          \
   }                                                                                          \
-  double refx_cvr_time_##S(void* h, VT alpha, const VT* b, VT beta, int iters) {                \
+  double REFX_FN(cvr_time_##S)(void* h, VT alpha, const VT* b, VT beta, int iters) {                \
     auto* box = (FmtBox<spMtxCVR<VT>, VT>*)h;                                                  \
     std::memcpy(box->b.data(), b, box->b.size() * sizeof(VT));                                \
     return time_loop(box, iters, [&] {                                                       \
-      sparse_mv<VT, spMtxCVR, false>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,           \
+      sparse_mv<VT, spMtxCVR, REFX_SIMD>(SPARSE_OPERATION_NON_TRANSPOSE, alpha, box->A,           \
                                     sparse_matrix_descr{}, box->b, beta, box->y);            \
     });                                                                                      \
   }
 REFX_CVR(double, f64)
 REFX_CVR(float, f32)
+#endif
 
 }  // extern "C"

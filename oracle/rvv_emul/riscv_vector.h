@@ -2,11 +2,12 @@
 //
 // A scalar stand-in for the RISC-V Vector C intrinsics (RVV 1.0 intrinsic
 // API, the non-overloaded `__riscv_*` names) restricted to the operations
-// that the reference's RVV-only kernels use: src/rvv/spmv_mtx_csr5.cpp,
-// src/rvv/spmv_mtx_vnec.cpp and src/rvv/spmv_vhcc.cpp of RVVLASparse.  With
-// it those files compile unmodified for x86-64 (oracle/Makefile target
-// `ref-rvv`), so the oracle's restatements of the three kernels can be
-// checked against the reference's own code.  Nothing in the product path
+// that the reference's RVV kernels use: src/rvv/*.cpp of RVVLASparse (the
+// CSR5, VNEC and VHCC kernels, which exist only in that form, and the RVV
+// versions of the CRS, HCSR, SELL-C-sigma, LAV and CVR products).  With it
+// those files compile unmodified for x86-64 (oracle/Makefile target
+// `ref-rvv`), so the oracle's restatements can be checked against the
+// reference's own code.  Nothing in the product path
 // includes this header.
 //
 // Model: VLEN = RVV_EMUL_VLEN bits (default 256, the machine the reference's
@@ -80,6 +81,8 @@ typedef rve_v<uint64_t, RVE_N(64, 1, 1)> vuint64m1_t;
 typedef rve_v<uint64_t, RVE_N(64, 2, 1)> vuint64m2_t;
 typedef rve_v<uint64_t, RVE_N(64, 4, 1)> vuint64m4_t;
 typedef rve_v<uint64_t, RVE_N(64, 8, 1)> vuint64m8_t;
+typedef rve_v<uint16_t, RVE_N(16, 1, 4)> vuint16mf4_t;
+typedef rve_v<uint16_t, RVE_N(16, 1, 2)> vuint16mf2_t;
 typedef rve_v<uint16_t, RVE_N(16, 1, 1)> vuint16m1_t;
 typedef rve_v<uint8_t, RVE_N(8, 1, 1)> vuint8m1_t;
 typedef rve_b<(size_t)(RVV_EMUL_VLEN) / 4> vbool4_t;
@@ -120,26 +123,28 @@ RVE_SETVL(e64m8, 64, 8, 1)
   }
 
 // ----------------------------------------- indexed (byte offset) load/store
-#define RVE_INDEXED(S, V, T, IX, M)                                                           \
-  static inline V __riscv_vloxei32_v_##S(const T* base, IX bindex, size_t vl) {                \
+#define RVE_INDEXED(S, V, T, IX, M) RVE_INDEXED_W(32, S, V, T, IX, M)
+#define RVE_INDEXED_W(W, S, V, T, IX, M)                                                      \
+  static inline V __riscv_vloxei##W##_v_##S(const T* base, IX bindex, size_t vl) {             \
     vl = rve::avl(vl, rve::lanes<V>());                                                       \
     V r{};                                                                                    \
     for (size_t i = 0; i < vl; ++i)                                                           \
       r.e[i] = rve::ld<T>((const char*)base + bindex.e[i]);                                   \
     return r;                                                                                 \
   }                                                                                           \
-  static inline V __riscv_vloxei32_v_##S##_m(M mask, const T* base, IX bindex, size_t vl) {   \
+  static inline V __riscv_vloxei##W##_v_##S##_m(M mask, const T* base, IX bindex, size_t vl) {\
     vl = rve::avl(vl, rve::lanes<V>());                                                       \
     V r{};                                                                                    \
     for (size_t i = 0; i < vl; ++i)                                                           \
       if (mask.e[i]) r.e[i] = rve::ld<T>((const char*)base + bindex.e[i]);                    \
     return r;                                                                                 \
   }                                                                                           \
-  static inline void __riscv_vsoxei32_v_##S(T* base, IX bindex, V v, size_t vl) {              \
+  static inline void __riscv_vsoxei##W##_v_##S(T* base, IX bindex, V v, size_t vl) {           \
     vl = rve::avl(vl, rve::lanes<V>());                                                       \
     for (size_t i = 0; i < vl; ++i) rve::st<T>((char*)base + bindex.e[i], v.e[i]);            \
   }                                                                                           \
-  static inline void __riscv_vsoxei32_v_##S##_m(M mask, T* base, IX bindex, V v, size_t vl) { \
+  static inline void __riscv_vsoxei##W##_v_##S##_m(M mask, T* base, IX bindex, V v,           \
+                                                   size_t vl) {                               \
     vl = rve::avl(vl, rve::lanes<V>());                                                       \
     for (size_t i = 0; i < vl; ++i)                                                           \
       if (mask.e[i]) rve::st<T>((char*)base + bindex.e[i], v.e[i]);                           \
@@ -184,6 +189,10 @@ RVE_SETVL(e64m8, 64, 8, 1)
     V r = vd;                                                                                 \
     for (size_t i = 0; i < vl; ++i) r.e[i] = std::fma(vs1.e[i], vs2.e[i], vd.e[i]);           \
     return r;                                                                                 \
+  }                                                                                           \
+  /* tail undisturbed: elements past vl keep vd (as the plain form does here) */              \
+  static inline V __riscv_vfmacc_vv_##S##_tu(V vd, V vs1, V vs2, size_t vl) {                 \
+    return __riscv_vfmacc_vv_##S(vd, vs1, vs2, vl);                                           \
   }                                                                                           \
   static inline V __riscv_vfmacc_vf_##S(V vd, T rs1, V vs2, size_t vl) {                      \
     vl = rve::avl(vl, rve::lanes<V>());                                                       \
@@ -433,6 +442,8 @@ RVE_LOAD(32, u32m1, vuint32m1_t, uint32_t)
 RVE_LOAD(32, u32m2, vuint32m2_t, uint32_t)
 RVE_LOAD(32, u32m4, vuint32m4_t, uint32_t)
 RVE_LOAD(32, u32m8, vuint32m8_t, uint32_t)
+RVE_LOAD(16, u16mf4, vuint16mf4_t, uint16_t)
+RVE_LOAD(16, u16mf2, vuint16mf2_t, uint16_t)
 RVE_LOAD(16, u16m1, vuint16m1_t, uint16_t)
 RVE_LOAD(8, u8m1, vuint8m1_t, uint8_t)
 RVE_STORE(64, f64m1, vfloat64m1_t, double)
@@ -459,6 +470,10 @@ RVE_INDEXED(u32m2, vuint32m2_t, uint32_t, vuint32m2_t, vbool16_t)
 RVE_INDEXED(u32m4, vuint32m4_t, uint32_t, vuint32m4_t, vbool8_t)
 RVE_INDEXED(u32m8, vuint32m8_t, uint32_t, vuint32m8_t, vbool4_t)
 
+// index vector of EEW 16 (HCSR's uint16 block columns): EMUL = LMUL * 16 / SEW
+RVE_INDEXED_W(16, f64m1, vfloat64m1_t, double, vuint16mf4_t, vbool64_t)
+RVE_INDEXED_W(16, f32m1, vfloat32m1_t, float, vuint16mf2_t, vbool32_t)
+
 // gather index: same SEW, same LMUL
 RVE_FLOAT(f64m1, f64m1, vfloat64m1_t, vfloat64m1_t, f64, vbool64_t, vuint64m1_t)
 RVE_FLOAT(f64m2, f64m1, vfloat64m2_t, vfloat64m1_t, f64, vbool32_t, vuint64m2_t)
@@ -469,6 +484,8 @@ RVE_FLOAT(f32m2, f32m1, vfloat32m2_t, vfloat32m1_t, f32, vbool16_t, vuint32m2_t)
 RVE_FLOAT(f32m4, f32m1, vfloat32m4_t, vfloat32m1_t, f32, vbool8_t, vuint32m4_t)
 RVE_FLOAT(f32m8, f32m1, vfloat32m8_t, vfloat32m1_t, f32, vbool4_t, vuint32m8_t)
 
+RVE_UINT(u16mf4, vuint16mf4_t, uint16_t, vbool64_t)
+RVE_UINT(u16mf2, vuint16mf2_t, uint16_t, vbool32_t)
 RVE_UINT(u32mf2, vuint32mf2_t, uint32_t, vbool64_t)
 RVE_UINT(u32m1, vuint32m1_t, uint32_t, vbool32_t)
 RVE_UINT(u32m2, vuint32m2_t, uint32_t, vbool16_t)

@@ -11,7 +11,9 @@ multiply-adds, its reductions, its thread split), so the check is normwise,
 at the restatement tolerances (1e-12 fp64, 1e-5 fp32), against the
 restatement and against the long-double CSR oracle.  The reference defects
 met on the way are pinned as such (CSR5 sigma > omega, VNEC-D rows spanning
-threads)."""
+threads).  The reference's RVV versions of the CRS, HCSR, SELL-C-sigma and
+LAV products (sparse_mv<T, Fmt, true>, its default) are checked the same
+way at the end."""
 import numpy as np
 import pytest
 
@@ -197,3 +199,45 @@ def test_vnec_ird_and_variant_match_reference_single_thread(dt):
         assert info["threads"] == 1
         assert abs(info["IRD_mat"] - float(ours["IRD_mat"])) <= 1e-6 * max(1.0, abs(info["IRD_mat"]))
         assert info["vnec_t"] == int(ours["vnec_t"])
+
+
+# ------------------------------------------- the reference's simd = true path
+def test_rvv_library_has_no_simd_cvr():
+    """src/rvv/spmv_mtx_cvr.cpp holds the scalar CVR product again (simd =
+    false only), so the RVV build exports no CVR entry points."""
+    L = O._ref(simd=True)
+    assert not hasattr(L, "refr_cvr_spmv_f64") and hasattr(L, "refr_crs_spmv_f64")
+
+
+def test_rvv_products_golden(g):
+    """sparse_mv<T, Fmt, true> — the reference's default — for CRS, HCSR,
+    SELL-C-sigma and LAV (src/rvv/spmv_mtx_{crs,hcsr,sell_c_sigma,lav}.cpp)
+    on the oracle's layouts, against the restatement and the long-double
+    oracle."""
+    dt = g["Val"].dtype
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    a, x, be, y0 = g["alpha"], g["x"], g["beta"], g["y0"]
+    yld = O.crs_spmv_ld(src, a, x, be, y0)
+    hb, sb, lb = O.build_hcsr(src, 64, 128), O.build_sell(src, 32, 256), O.build_lav(src, 8, 0.2, 40000)
+    for name, ref, mine in (("crs", O.ref_crs(src, simd=True), src), ("hcsr", O.ref_hcsr(hb, simd=True), hb),
+                            ("sell", O.ref_sell(sb, simd=True), sb), ("lav", O.ref_lav(lb, simd=True), lb)):
+        yr = ref.spmv(a, x, be, y0)
+        assert O.normwise_relerr(yr, O.spmv(mine, a, x, be, y0)) < tol_for(dt), name
+        assert O.normwise_relerr(yr, yld) < tol_for(dt), name
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_rvv_products_powerlaw(dt):
+    m, n, R, C, V = W.powerlaw(3000, seed=3)
+    src = O.crs(m, n, R, C, V.astype(dt))
+    x, y0 = W.vector(n, 0).astype(dt), W.vector(m, 1).astype(dt)
+    yld = O.crs_spmv_ld(src, 1.25, x, 0.5, y0)
+    for R_, C_ in ((256, 256), (2000, 2000)):
+        hb = O.build_hcsr(src, R_, C_)
+        assert O.normwise_relerr(O.ref_hcsr(hb, simd=True).spmv(1.25, x, 0.5, y0), yld) < tol_for(dt)
+    for C_, sigma in ((8, 1), (32, 256)):
+        sb = O.build_sell(src, C_, sigma)
+        assert O.normwise_relerr(O.ref_sell(sb, simd=True).spmv(1.25, x, 0.5, y0), yld) < tol_for(dt)
+    assert O.normwise_relerr(O.ref_crs(src, simd=True).spmv(1.25, x, 0.5, y0), yld) < tol_for(dt)
+    lb = O.build_lav(src, 8, 0.2, 1000)
+    assert O.normwise_relerr(O.ref_lav(lb, simd=True).spmv(1.25, x, 0.5, y0), yld) < tol_for(dt)
