@@ -466,6 +466,7 @@ def _refv():
         L.refv_last_error.restype = C.c_char_p
         L.refv_num_threads.restype = cint
         L.refv_vlen.restype = cint
+        L.refv_selftest.restype = cint
         for S, T in (("f64", dbl), ("f32", flt)):
             def p(name, res, args):
                 f = getattr(L, name.replace("@", S))

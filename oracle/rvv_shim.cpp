@@ -19,6 +19,7 @@
 #include "sparse_matrix.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -67,6 +68,69 @@ int run(M& box, T alpha, const T* b, T beta, T* y, Fn&& call) {
 extern "C" {
 
 const char* refv_last_error() { return g_last_error.c_str(); }
+
+// Known answers for the intrinsic stand-in (values worked out by hand from the
+// RVV 1.0 intrinsic definitions); returns 0, or the number of the first check
+// that failed.
+int refv_selftest() {
+  int k = 0;
+#define REFV_CHECK(cond) \
+  do {                   \
+    ++k;                 \
+    if (!(cond)) return k; \
+  } while (0)
+  // VLMAX at VLEN 256
+  REFV_CHECK(__riscv_vsetvlmax_e64m2() == 8 && __riscv_vsetvlmax_e32m2() == 16 &&
+             __riscv_vsetvlmax_e64m8() == 32 && __riscv_vsetvl_e64m2(5) == 5 && __riscv_vsetvl_e64m2(50) == 8);
+  // mask bit i = bit i of the register image, LSB first
+  const uint8_t bytes[32] = {0x05, 0x80};
+  vbool32_t m = __riscv_vreinterpret_v_u8m1_b32(__riscv_vle8_v_u8m1(bytes, 2));
+  REFV_CHECK(m.e[0] == 1 && m.e[1] == 0 && m.e[2] == 1 && m.e[7] == 0 && __riscv_vcpop_m_b32(m, 8) == 2);
+  // viota: set elements below i
+  vuint32m1_t io = __riscv_viota_m_u32m1(m, 8);
+  REFV_CHECK(io.e[0] == 0 && io.e[1] == 1 && io.e[2] == 1 && io.e[3] == 2 && io.e[7] == 2);
+  // vcompress packs the active elements to the front
+  const double v8[8] = {10, 11, 12, 13, 14, 15, 16, 17};
+  vfloat64m2_t a = __riscv_vle64_v_f64m2(v8, 8);
+  vfloat64m2_t c = __riscv_vcompress_vm_f64m2(a, m, 8);
+  REFV_CHECK(c.e[0] == 10 && c.e[1] == 12);
+  // slides
+  vfloat64m2_t d = __riscv_vfslide1down_vf_f64m2(a, -1.0, 8);
+  REFV_CHECK(d.e[0] == 11 && d.e[6] == 17 && d.e[7] == -1);
+  vfloat64m2_t u = __riscv_vslideup_vx_f64m2(__riscv_vfmv_v_f_f64m2(0.0, 8), a, 3, 8);
+  REFV_CHECK(u.e[2] == 0 && u.e[3] == 10 && u.e[7] == 14);
+  // gather: an index at or past VLMAX reads 0
+  const uint32_t gi32[8] = {7, 0, 8, 1, 100, 2, 3, 4};
+  vuint64m2_t gi = __riscv_vwcvtu_x_x_v_u64m2(__riscv_vle32_v_u32m1(gi32, 8), 8);
+  vfloat64m2_t gth = __riscv_vrgather_vv_f64m2(a, gi, 8);
+  REFV_CHECK(gth.e[0] == 17 && gth.e[1] == 10 && gth.e[2] == 0 && gth.e[4] == 0 && gth.e[7] == 14);
+  // masked-undisturbed add keeps maskedoff where the mask is 0
+  vfloat64m2_t off = __riscv_vfmv_v_f_f64m2(-5.0, 8);
+  vfloat64m2_t mu = __riscv_vfadd_vv_f64m2_mu(m, off, a, a, 8);
+  REFV_CHECK(mu.e[0] == 20 && mu.e[1] == -5 && mu.e[2] == 24 && mu.e[3] == -5);
+  // vfmacc is fused: (1 + 2^-30)^2 - (1 + 2^-29) keeps the 2^-60 term
+  const double e = 1.0 + std::ldexp(1.0, -30);
+  vfloat64m2_t acc = __riscv_vfmv_v_f_f64m2(-(1.0 + std::ldexp(1.0, -29)), 1);
+  acc = __riscv_vfmacc_vf_f64m2(acc, e, __riscv_vfmv_v_f_f64m2(e, 1), 1);
+  REFV_CHECK(acc.e[0] == std::ldexp(1.0, -60));
+  // reductions start from the scalar operand's element 0
+  vfloat64m1_t s0 = __riscv_vfmv_v_f_f64m1(100.0, 1);
+  REFV_CHECK(__riscv_vfmv_f_s_f64m1_f64(__riscv_vfredusum_vs_f64m2_f64m1(a, s0, 8)) == 100 + 108);
+  // indexed loads take byte offsets; a vl above VLMAX acts as VLMAX
+  const uint32_t boff[8] = {8, 0, 56, 16, 0, 0, 0, 0};
+  vfloat64m2_t ix = __riscv_vloxei32_v_f64m2(v8, __riscv_vle32_v_u32m1(boff, 4), 4);
+  REFV_CHECK(ix.e[0] == 11 && ix.e[1] == 10 && ix.e[2] == 17 && ix.e[3] == 12);
+  vfloat64m1_t cl = __riscv_vfmv_v_f_f64m1(3.0, 64);
+  REFV_CHECK(cl.e[0] == 3 && cl.e[3] == 3);
+  // unsigned compare, masked integer add
+  vuint32m1_t p = __riscv_vle32_v_u32m1(gi32, 8);
+  vbool32_t le = __riscv_vmsleu_vv_u32m1_b32(p, __riscv_vmv_v_x_u32m1(7, 8), 8);
+  REFV_CHECK(le.e[0] == 1 && le.e[2] == 0 && le.e[4] == 0 && __riscv_vcpop_m_b32(le, 8) == 6);
+  vuint32m1_t pa = __riscv_vadd_vx_u32m1_mu(le, p, p, 1000u, 8);
+  REFV_CHECK(pa.e[0] == 1007 && pa.e[2] == 8 && pa.e[4] == 100);
+#undef REFV_CHECK
+  return 0;
+}
 int refv_num_threads() { return omp_get_max_threads(); }
 int refv_vlen() { return RVV_EMUL_VLEN; }
 

@@ -35,6 +35,13 @@ def omegas(dt):
     return [O.refv_lanes(sew, k) for k in (1, 2, 4, 8)]
 
 
+def test_stand_in_known_answers():
+    """oracle/rvv_shim.cpp refv_selftest: mask bit order, viota, vcompress,
+    slides, out-of-range gathers, mask-undisturbed adds, the fused vfmacc,
+    reductions, byte-offset indexed loads, the vl clamp (0 = all hold)."""
+    assert O._refv().refv_selftest() == 0
+
+
 def test_stand_in_vector_lengths():
     assert O.refv_vlen() == 256
     assert omegas(np.float64) == [4, 8, 16, 32] and omegas(np.float32) == [8, 16, 32, 64]
