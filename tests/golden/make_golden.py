@@ -11,6 +11,13 @@ reference SELL-C-sigma / LAV / CVR kernels run on the layouts our builders
 produce (layout arrays stored too).  Inputs come from the library's seeded
 generators; the fixtures are what tests compare against, so they are never
 regenerated at test time.
+
+Also stored (``add_rvv_outputs``; ``--rvv-only`` adds them to existing
+fixtures without touching their other keys): the reference's RVV-only
+kernels, built from its src/rvv/ sources on the oracle's intrinsic stand-in
+(VLEN 256), run on the oracle builders' layouts — CSR5 (omega 32, sigma 16),
+VHCC (3 threads, 8 fp64 / 16 fp32 lanes) and VNEC D, S and L (one thread,
+so none of the reference's multi-thread defects applies).
 """
 import os
 import sys
@@ -81,10 +88,35 @@ def main():
             for k, v in cv.arrays.items():
                 d["cvr_" + k] = v
             d["cvr_y"] = O.ref_cvr(cv).spmv(alpha, x, beta, y0)
+            rvv_outputs(A, d)
             fn = os.path.join(OUT, f"{name}_{'f64' if dt == np.float64 else 'f32'}.npz")
             np.savez_compressed(fn, **d)
             print("wrote", os.path.relpath(fn, ROOT), os.path.getsize(fn))
 
 
+def rvv_outputs(A, d):
+    """Adds the reference RVV kernels' outputs for the fixture's inputs to d."""
+    alpha, beta, x, y0 = float(d["alpha"]), float(d["beta"]), d["x"], d["y0"]
+    lanes = 8 if A.dtype == np.float64 else 16
+    d["csr5_omega"], d["csr5_sigma"] = 32, 16
+    d["csr5_y"] = O.refv_csr5(O.build_csr5(A, 32, 16)).spmv(alpha, x, beta, y0)
+    d["vhcc_threads"], d["vhcc_lanes"] = 3, lanes
+    d["vhcc_y"] = O.refv_vhcc(O.build_vhcc(A, 3, lanes)).spmv(alpha, x, beta, y0)
+    for variant in (0, 1, 2):
+        d[f"vnec{variant}_y"] = O.refv_vnec(A, O.build_vnec(A, 1, variant)).spmv(alpha, x, beta, y0)
+
+
+def add_rvv_outputs():
+    O.build(ref=True)
+    for fn in sorted(f for f in os.listdir(OUT) if f.endswith(".npz")):
+        path = os.path.join(OUT, fn)
+        with np.load(path) as z:
+            d = {k: z[k] for k in z.files}
+        A = O.crs(int(d["m"]), int(d["n"]), d["Rst"], d["Col"], d["Val"])
+        rvv_outputs(A, d)
+        np.savez_compressed(path, **d)
+        print("updated", os.path.relpath(path, ROOT), os.path.getsize(path))
+
+
 if __name__ == "__main__":
-    main()
+    add_rvv_outputs() if "--rvv-only" in sys.argv[1:] else main()

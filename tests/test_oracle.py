@@ -136,3 +136,21 @@ def test_transpose_and_sddmm_definitions(g):
     gv = np.linspace(-1, 1, m)
     dv = O.sddmm(A, gv, g["x"])
     assert np.array_equal(dv, gv[rows] * g["x"].astype(np.float64)[g["Col"]])
+
+
+def test_rvv_kernel_fixtures(g):
+    """The reference's RVV-only kernels' outputs stored in the fixtures
+    (tests/golden/make_golden.py, rvv_outputs: CSR5 omega 32 / sigma 16, VHCC,
+    VNEC D/S/L on one thread, all on the oracle builders' layouts) against the
+    restatements — the pin that holds where the reference sources are absent."""
+    dt = g["Val"].dtype
+    src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
+    a, x, be, y0 = g["alpha"], g["x"], g["beta"], g["y0"]
+    tol = tol_for(dt)
+    c5 = O.build_csr5(src, int(g["csr5_omega"]), int(g["csr5_sigma"]))
+    assert O.normwise_relerr(O.spmv(c5, a, x, be, y0), g["csr5_y"]) < tol
+    vh = O.build_vhcc(src, int(g["vhcc_threads"]), int(g["vhcc_lanes"]))
+    assert O.normwise_relerr(O.spmv(vh, a, x, be, y0), g["vhcc_y"]) < tol
+    for variant in (0, 1, 2):
+        vn = O.build_vnec(src, 1, variant)
+        assert O.normwise_relerr(O.spmv(vn, a, x, be, y0), g[f"vnec{variant}_y"]) < tol, variant

@@ -85,8 +85,8 @@ def test_csr5_reference_sigma_above_omega_skips_part_of_single_row_tiles():
     (omega, sigma) (src/rvv/spmv_mtx_csr5.cpp:161-163 against :44-46): with
     sigma > omega it asks for sigma lanes per step, gets omega (VLMAX), and
     steps sigma elements, so a tile that lies inside one row loses part of its
-    sum.  The restatement sums the whole tile; the GPU path only uses
-    sigma <= omega = 32."""
+    sum.  The restatement and the GPU kernels sum the whole tile (the GPU
+    tests include sigma 40 > omega 32); only sigma <= omega is pinned."""
     g = load_golden([p for p in GOLD if "one_long_row_f64" in p][0])
     src = O.crs(g["m"], g["n"], g["Rst"], g["Col"], g["Val"])
     b = O.build_csr5(src, 4, 16)
