@@ -493,7 +493,7 @@ int rvvla_csr5_spmv_mixed(const rvvla_csr5* A, int val_type, float alpha, const 
  * device resolves that array's address (and may load the module): make it
  * before any stream capture.  Calls overlapping in time on one device share
  * the array and race: serialise them.  Always runs the register-staged
- * kernel. */
+ * kernel, whatever RVVLA_CSR5_STAGING selects for the ordinary entry. */
 int rvvla_csr5_spmv_f64_noalloc(const rvvla_csr5* A, double alpha, const double* x, double beta,
                                 double* y, void* stream);
 

@@ -30,7 +30,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_scalar.so")
 REFV_LIB = os.path.join(HERE, "_ref", "libref_rvv.so")
-REF_SRC = os.environ.get("RVVLA_REFERENCE_SRC", "/root/reference")
+# The reference checkout: RVVLA_REFERENCE_SRC, else a "reference" directory
+# beside the repository.  Only building oracle/_ref reads it.
+REF_SRC = os.environ.get("RVVLA_REFERENCE_SRC",
+                         os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
 
 I32, U32, U16, U8, F32, F64, I64, U64 = range(8)
 _NP = {I32: np.int32, U32: np.uint32, U16: np.uint16, U8: np.uint8, F32: np.float32, F64: np.float64,

@@ -654,10 +654,18 @@ int csr5_validate(const rvvla_csr5* A, const void* x, const void* y) {
 // gets an equal share of tiles), so no partial second wave trails the grid.
 template <class V, class X, class Ac, class CT>
 int c5_resident_warps(int sigma, int mode) {
-  static int cache[4][3] = {};
+  // per device (GPUs of one machine may differ), written once per entry;
+  // concurrent first calls compute the same value
+  constexpr int kDev = 16;
+  static std::atomic<int> cache[kDev][4][3];  // static storage: zero-initialised
   const int si = sigma / 8 - 1;
   if (si < 0 || si > 3 || sigma % 8 || mode < 0 || mode > 2) return 48;
-  int& c = cache[si][mode];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDev) {
+    cudaGetLastError();
+    dev = -1;
+  }
+  int c = dev >= 0 ? cache[dev][si][mode].load(std::memory_order_relaxed) : 0;
   if (c == 0) {
     int blocks = 0;
     cudaError_t e = cudaErrorInvalidValue;
@@ -680,6 +688,8 @@ int c5_resident_warps(int sigma, int mode) {
 #undef C5_OCC
     }
     c = (e == cudaSuccess && blocks > 0) ? std::min(48, blocks * kC5Warps) : 48;
+    if (e != cudaSuccess) cudaGetLastError();
+    if (dev >= 0) cache[dev][si][mode].store(c, std::memory_order_relaxed);
   }
   return c;
 }
@@ -702,8 +712,9 @@ int csr5_spmv_impl(const rvvla_csr5* A, X alpha, const X* x, X beta, X* y, cudaS
     // register-only kernel
     const bool aligned = ((uintptr_t)A->csr_value % 16 == 0) && ((uintptr_t)A->csr_column_index % 16 == 0) &&
                          ((uintptr_t)A->tile_descriptor % 16 == 0);
-    int mode = csr5_staging();
-    if (regs_only && mode == kC5Tma) mode = kC5Regs;
+    // regs_only: the register-staged kernel whatever the staging knob says
+    // (no TMA ring, no doubled register set)
+    const int mode = regs_only ? kC5Regs : csr5_staging();
     const int per_sm = aligned ? c5_resident_warps<V, X, Ac, CT>(A->sigma, mode) : 48;
     const int64_t want_warps = (int64_t)sm_count() * per_sm;
     int tpw = (int)std::max<int64_t>(1, (nfull + want_warps - 1) / want_warps);
