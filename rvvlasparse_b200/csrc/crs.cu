@@ -42,6 +42,13 @@
 
 namespace rvvla {
 
+// Row-start bitmap: bit rst[r] for every row r with nonzeros.
+__global__ void crs_run_bits_kernel(int m, const int* __restrict__ rst, uint32_t* __restrict__ bits) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < m && rst[r + 1] > rst[r]) atomicOr(bits + (rst[r] >> 5), 1u << (rst[r] & 31));
+}
+
+
 // Nonzeros per warp in the stream and lane-run kernels: 2048, halved (down
 // to 256) while the matrix would give fewer than ~6 waves of 4736 warps (148
 // SMs x 32 resident warps), so a medium-size matrix does not leave a large

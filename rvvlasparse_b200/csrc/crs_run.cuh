@@ -253,10 +253,4 @@ crs_run_kernel(int m, int nnz, int E, int nwarps, const int* __restrict__ rst, c
   }
 }
 
-// Row-start bitmap: bit rst[r] for every row r with nonzeros.
-__global__ void crs_run_bits_kernel(int m, const int* __restrict__ rst, uint32_t* __restrict__ bits) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < m && rst[r + 1] > rst[r]) atomicOr(bits + (rst[r] >> 5), 1u << (rst[r] & 31));
-}
-
 }  // namespace rvvla

@@ -1,0 +1,572 @@
+// hcsr_spmv.cu — y = alpha*A*x + beta*y for spMtxHCSR on sm_100a.
+//
+// Reference: src/scalar/spmv_mtx_hcsr.cpp:22-134.  The reference walks a
+// block row's blocks in block-column order and adds every block's
+// contribution into y[block row]: a CSR block (kind 1) adds one row sum per
+// row, a COO block (any other kind) adds one product per nonzero.  Any R and
+// C are accepted (the only limits are the format's: uint16 local columns,
+// 30-bit row_ptr offsets).
+//
+// GPU mapping.  One CTA of 16 warps per block row; the block row's R partial
+// sums live in shared memory (or, for block rows too tall for shared memory,
+// in a global scratch slice the CTA owns).  Every row belongs to one warp:
+// warp w owns rows [ceil(w*rows/16), ceil((w+1)*rows/16)), so no two warps
+// ever add into the same row and the summation order of every row is fixed —
+// the result is bitwise reproducible run to run (no float atomics).
+//
+// The block columns are taken in windows of kHWin blocks: the window's
+// non-empty blocks are compacted into a CSR list and a COO list in shared
+// memory (so the metadata staged never depends on b_n), then
+//   * CSR phase: each warp walks every CSR block of the window for its own
+//     rows: their nonzeros are one contiguous range, streamed in chunks of
+//     256 (8 consecutive nonzeros per lane, 16-byte loads of values and
+//     uint16 columns); the rows starting inside a chunk are marked from the
+//     block's row_ptr (a window of 32 row starts per lane set, prefetched one
+//     window ahead), each lane sums its 8 products split at the marks, and a
+//     reverse segmented warp scan closes the rows that cross lanes, so each
+//     row piece of a chunk is added to the accumulator exactly once;
+//   * COO phase: the window's COO nonzeros (all COO blocks, in block order)
+//     are cut into rounds of 2048; every warp computes 128 products in stream
+//     order (the block of each nonzero from the compacted list: a warp-wide
+//     OR of the next block starts and a popcount), writes (row, product,
+//     owner) to shared memory, and after a barrier each owner warp picks its
+//     own nonzeros in stream order and adds them (nonzeros of one row inside a
+//     group of 32 are summed in lane order first).
+// The next round's loads are issued before the current round is applied.
+// Per row, the sum is: CSR pieces of window 0 in block order, COO products of
+// window 0 in stream order, then window 1, ...; y = alpha*acc + beta*y at the
+// end (y is not read when beta == 0).
+//
+// Mixed forms: lane sums of the CSR phase in compensated fp32 (two-sum), COO
+// products in fp32; the block-row accumulator, where pieces of different
+// blocks meet, is fp64.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <type_traits>
+
+#include "crs_merge.cuh"
+#include "crs_run.cuh"
+#include "rvvla_internal.cuh"
+
+namespace rvvla {
+namespace {
+
+constexpr uint32_t kHKindMask = 0x3FFFFFFFu;
+constexpr int kHT = 512;                   // threads per CTA
+constexpr int kHW = kHT / 32;              // warps = row owners
+constexpr int kHWin = 2048;                // block columns per window
+constexpr int kHRound = 2048;              // COO nonzeros per round
+constexpr int kHU = kHRound / (kHW * 32);  // sub-steps of 32 per warp and round
+constexpr int kHLane = 8;                  // CSR nonzeros per lane and chunk
+constexpr int kHChunk = 32 * kHLane;
+
+// a non-empty block of the window: COO stream start (COO list only), nonzero
+// offset, row_ptr offset, block column
+struct HBlk {
+  int cs;
+  int bp;
+  uint32_t off;
+  int j;
+};
+static_assert(sizeof(HBlk) == 16, "HBlk is one 16-byte shared-memory load");
+
+__host__ __device__ constexpr size_t hal16(size_t b) { return (b + 15) / 16 * 16; }
+
+// Dynamic shared memory: [acc] list | prod | row | own | per-warp scratch |
+// per-warp mark groups.
+template <class SA, class P>
+struct HLayout {
+  size_t acc, list, prod, row, own, wscr, mgrp, total;
+  __host__ __device__ explicit HLayout(int64_t racc) {
+    acc = 0;
+    list = hal16((size_t)racc * sizeof(SA));
+    prod = list + hal16((size_t)(kHWin + 1) * sizeof(HBlk));
+    row = prod + hal16((size_t)kHRound * sizeof(P));
+    own = row + (size_t)kHRound * 4;
+    wscr = own + hal16((size_t)kHRound);
+    mgrp = wscr + (size_t)kHW * 1024;
+    total = mgrp + (size_t)kHW * 32 * 4;
+  }
+};
+
+template <class V, class X, class SA, bool MIX>
+struct HTypes {
+  using Ac = std::conditional_t<MIX, CompF32, SA>;                        // CSR lane sums
+  using P = std::conditional_t<(MIX || sizeof(SA) == 4), float, double>;  // a COO product
+  using PT = decltype(vmul(V(), X()));                                    // a CSR product
+};
+
+// Exclusive CTA-wide scan of three counters; t* are the CTA totals.
+__device__ __forceinline__ void hcsr_scan3(int a, int b, int c, int& pa, int& pb, int& pc, int& ta, int& tb,
+                                           int& tc, int* s_w) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int ia = a, ib = b, ic = c;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int oa = __shfl_up_sync(0xffffffffu, ia, d);
+    const int ob = __shfl_up_sync(0xffffffffu, ib, d);
+    const int oc = __shfl_up_sync(0xffffffffu, ic, d);
+    if (lane >= d) {
+      ia += oa;
+      ib += ob;
+      ic += oc;
+    }
+  }
+  if (lane == 31) {
+    s_w[warp] = ia;
+    s_w[kHW + warp] = ib;
+    s_w[2 * kHW + warp] = ic;
+  }
+  __syncthreads();
+  int wa = 0, wb = 0, wc = 0;
+  ta = tb = tc = 0;
+#pragma unroll
+  for (int w = 0; w < kHW; ++w) {
+    const int va = s_w[w], vb = s_w[kHW + w], vc = s_w[2 * kHW + w];
+    if (w < warp) {
+      wa += va;
+      wb += vb;
+      wc += vc;
+    }
+    ta += va;
+    tb += vb;
+    tc += vc;
+  }
+  pa = wa + ia - a;
+  pb = wb + ib - b;
+  pc = wc + ic - c;
+  __syncthreads();
+}
+
+// eight uint16 columns with one 16-byte load
+__device__ __forceinline__ void hcsr_cols8(const uint16_t* p, uint32_t (&c)[kHLane], uint64_t pol) {
+  const int4 t = ld_v4_l1(p, pol);
+  const uint32_t w[4] = {(uint32_t)t.x, (uint32_t)t.y, (uint32_t)t.z, (uint32_t)t.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    c[2 * q] = w[q] & 0xFFFFu;
+    c[2 * q + 1] = w[q] >> 16;
+  }
+}
+
+template <class V>
+__device__ __forceinline__ V hcsr_ld1(const V* p) {
+  if constexpr (std::is_same_v<V, __nv_bfloat16>) return __ushort_as_bfloat16(__ldg((const unsigned short*)p));
+  else return __ldg(p);
+}
+
+template <class SA, class T>
+__device__ __forceinline__ void hcsr_add(SA* acc, int r, T v) {
+  acc[r] += (SA)v;
+}
+
+// CSR phase of one warp for one CSR block: rows [ra, rb) of the block, whose
+// nonzeros are [lo, hi) (absolute).  Row starts come from rp (the block's
+// row_ptr, block-relative) in windows of 32 rows.
+template <class V, class X, class SA, bool MIX, bool VEC>
+__device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t lo,
+                                              int64_t hi, int64_t nz, const uint16_t* __restrict__ col_idx,
+                                              const V* __restrict__ values, const X* __restrict__ xb, SA* acc,
+                                              int* table, uint32_t* mgrp, int lane, uint64_t pf, uint64_t pl) {
+  using Ty = HTypes<V, X, SA, MIX>;
+  using Ac = typename Ty::Ac;
+  using PT = typename Ty::PT;
+  using CT = SA;
+  // row window: lane l holds the starts of rows wb + l and wb + l + 1 (the
+  // next window is loaded one window ahead)
+  int wb = ra;
+  auto ldwin = [&](int base, uint32_t& s, uint32_t& e) {
+    const int r = base + lane;
+    s = r < rb ? __ldg(rp + r) : 0xFFFFFFFFu;
+    e = r < rb ? __ldg(rp + r + 1) : 0xFFFFFFFFu;
+  };
+  uint32_t s_c, e_c, s_n, e_n;
+  ldwin(wb, s_c, e_c);
+  ldwin(wb + 32, s_n, e_n);
+  int open_row = -1;
+  for (int64_t c = lo & ~(int64_t)7; c < hi; c += kHChunk) {
+    const int64_t a = c + kHLane * lane;
+    // ---- loads and products
+    PT p[kHLane];
+    {
+      V vv[kHLane];
+      uint32_t cc[kHLane];
+      const bool any = a < hi && a + kHLane > lo;
+      if (VEC && any && a + kHLane <= nz) {
+        RunVec<V>::load(values + a, vv, pf);
+        hcsr_cols8(col_idx + a, cc, pf);
+      } else {
+#pragma unroll
+        for (int i = 0; i < kHLane; ++i) {
+          const bool ok = a + i >= lo && a + i < hi;
+          vv[i] = ok ? hcsr_ld1(values + a + i) : V(0);
+          cc[i] = ok ? (uint32_t)__ldg(col_idx + a + i) : 0u;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) {
+        const bool ok = a + i >= lo && a + i < hi;
+        if constexpr (MIX) p[i] = ok ? to_f32(vv[i]) * (float)ld_keep(xb + cc[i], pl) : 0.f;
+        else p[i] = ok ? vv[i] * ld_keep(xb + cc[i], pl) : PT(0);
+      }
+    }
+    // ---- marks of the rows that start inside the chunk
+    mgrp[lane] = 0u;
+    __syncwarp();
+    for (;;) {
+      const int64_t pos = bp + (int64_t)s_c - c;
+      if (wb + lane < rb && pos >= 0 && pos < kHChunk && s_c < e_c) {
+        table[pos] = wb + lane;
+        atomicOr(mgrp + (pos >> 3), 1u << (pos & 7));
+      }
+      const uint32_t s31 = __shfl_sync(0xffffffffu, s_c, 31);
+      const bool exhausted = wb + 32 < rb && bp + (int64_t)s31 - c < kHChunk;
+      if (!exhausted) break;
+      wb += 32;
+      s_c = s_n;
+      e_c = e_n;
+      ldwin(wb + 32, s_n, e_n);
+    }
+    __syncwarp();
+    const uint32_t mb = mgrp[lane];
+    // ---- lane sums split at the marks; rows closed inside the lane are added now
+    Ac sum, lead;
+    acc_zero(sum);
+    acc_zero(lead);
+    int nf = 0, rcur = -1;
+#pragma unroll
+    for (int i = 0; i < kHLane; ++i) {
+      if ((mb >> i) & 1u) {
+        if (nf == 0) lead = sum;
+        else hcsr_add(acc, rcur, acc_carry(sum));
+        rcur = table[kHLane * lane + i];
+        ++nf;
+        acc_zero(sum);
+      }
+      acc_add(sum, p[i]);
+    }
+    if (nf == 0) lead = sum;
+    // ---- rows crossing lanes: reverse segmented scan of the leads
+    const unsigned marks = __ballot_sync(0xffffffffu, nf > 0);
+    const unsigned ge = marks & (~0u << lane);
+    const int e = ge ? __ffs(ge) - 1 : 31;
+    CT T = (CT)acc_carry(lead);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const CT o = __shfl_down_sync(0xffffffffu, T, d);
+      if (lane + d <= e) T += o;
+    }
+    CT Tn = __shfl_down_sync(0xffffffffu, T, 1);
+    if (lane == 31) Tn = CT(0);
+    const CT T0 = __shfl_sync(0xffffffffu, T, 0);
+    if (lane == 0 && open_row >= 0) hcsr_add(acc, open_row, T0);
+    if (nf > 0) hcsr_add(acc, rcur, (CT)acc_carry(sum) + Tn);
+    if (marks) open_row = __shfl_sync(0xffffffffu, rcur, 31 - __clz(marks));
+    __syncwarp();
+  }
+}
+
+// Raw loads of one COO sub-step (32 consecutive COO nonzeros of the window).
+template <class V>
+struct HCooRaw {
+  uint32_t row;
+  uint32_t col;
+  V v;
+  int64_t xoff;
+  bool ok;
+};
+
+template <class V, class X, class SA, bool MIX, bool VEC, bool GACC>
+__global__ void __launch_bounds__(kHT, 2)
+hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const int* __restrict__ block_ptr,
+                 const uint32_t* __restrict__ row_offset, const uint32_t* __restrict__ row_ptr,
+                 const uint16_t* __restrict__ col_idx, const V* __restrict__ values, const X* __restrict__ x,
+                 X* __restrict__ y, X alpha, X beta, SA* __restrict__ gacc) {
+  using Ty = HTypes<V, X, SA, MIX>;
+  using P = typename Ty::P;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_w[3 * kHW];
+  const HLayout<SA, P> L(GACC ? 0 : R);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t br = blockIdx.x;
+  const int64_t r0 = br * R;
+  const int rows = (int)min(R, m - r0);
+  SA* acc = GACC ? gacc + r0 : reinterpret_cast<SA*>(smem + L.acc);
+  HBlk* list = reinterpret_cast<HBlk*>(smem + L.list);
+  P* s_prod = reinterpret_cast<P*>(smem + L.prod);
+  uint32_t* s_row = reinterpret_cast<uint32_t*>(smem + L.row);
+  uint8_t* s_own = smem + L.own;
+  int* table = reinterpret_cast<int*>(smem + L.wscr + (size_t)warp * 1024);          // CSR phase
+  uint16_t* olist = reinterpret_cast<uint16_t*>(smem + L.wscr + (size_t)warp * 1024);  // COO phase
+  uint32_t* mgrp = reinterpret_cast<uint32_t*>(smem + L.mgrp) + warp * 32;
+  const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+
+  for (int li = tid; li < rows; li += kHT) acc[li] = SA(0);
+  // this warp's rows
+  const int ra = (int)(((int64_t)warp * rows + kHW - 1) / kHW);
+  const int rb = (int)(((int64_t)(warp + 1) * rows + kHW - 1) / kHW);
+  const int64_t blk0 = br * b_n;
+  __syncthreads();
+
+  for (int64_t jw = 0; jw < b_n; jw += kHWin) {
+    const int nb = (int)(b_n - jw < kHWin ? b_n - jw : kHWin);
+    // ---- compact the window's non-empty blocks (4 consecutive per thread)
+    int bpq[4], cntq[4];
+    uint32_t roq[4];
+    int n_csr = 0, n_coo = 0, n_ent = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int jj = 4 * tid + q;
+      bpq[q] = 0;
+      cntq[q] = 0;
+      roq[q] = 0u;
+      if (jj < nb) {
+        const int64_t b = blk0 + jw + jj;
+        bpq[q] = block_ptr[b];
+        cntq[q] = block_ptr[b + 1] - bpq[q];
+        roq[q] = row_offset[b];
+        if (cntq[q] > 0) {
+          if ((roq[q] >> 30) == 1u) ++n_csr;
+          else {
+            ++n_coo;
+            n_ent += cntq[q];
+          }
+        }
+      }
+    }
+    int p_csr, p_coo, p_ent, t_csr, t_coo, t_ent;
+    hcsr_scan3(n_csr, n_coo, n_ent, p_csr, p_coo, p_ent, t_csr, t_coo, t_ent, s_w);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (cntq[q] > 0) {
+        HBlk h;
+        h.bp = bpq[q];
+        h.off = roq[q] & kHKindMask;
+        h.j = (int)(jw + 4 * tid + q);
+        if ((roq[q] >> 30) == 1u) {
+          h.cs = 0;
+          list[kHWin + 1 - t_csr + p_csr++] = h;
+        } else {
+          h.cs = p_ent;
+          p_ent += cntq[q];
+          list[p_coo++] = h;
+        }
+      }
+    }
+    if (tid == 0) list[t_coo].cs = t_ent;  // sentinel: end of the COO stream
+    __syncthreads();
+
+    // ---- CSR phase: this warp's rows of every CSR block of the window
+    if (ra < rb) {
+      for (int i = 0; i < t_csr; ++i) {
+        const HBlk h = list[kHWin + 1 - t_csr + i];
+        const uint32_t* rp = row_ptr + h.off;
+        const int64_t lo = (int64_t)h.bp + __ldg(rp + ra), hi = (int64_t)h.bp + __ldg(rp + rb);
+        if (lo >= hi) continue;
+        hcsr_csr_rows<V, X, SA, MIX, VEC>(rp, h.bp, ra, rb, lo, hi, nz, col_idx, values, x + (int64_t)h.j * C, acc,
+                                          table, mgrp, lane, pf, pl);
+      }
+    }
+
+    // ---- COO phase: rounds of kHRound nonzeros of the window's COO stream
+    if (t_ent > 0) {
+      const int ncoo = t_coo, ntot = t_ent;
+      const int nrounds = (ntot + kHRound - 1) / kHRound;
+      HCooRaw<V> raw[kHU];
+      auto coo_load = [&](int t) {
+        const int q00 = t * kHRound + warp * (kHU * 32);
+        int ia = 0;
+        if (lane == 0) {
+          const int qs = min(q00, ntot - 1);
+          int lo = 0, hi = ncoo;
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (list[mid].cs <= qs) lo = mid;
+            else hi = mid;
+          }
+          ia = lo;
+        }
+        ia = __shfl_sync(0xffffffffu, ia, 0);
+#pragma unroll
+        for (int u = 0; u < kHU; ++u) {
+          const int q0 = q00 + 32 * u;
+          const int nxt = ia + 1 + lane;
+          const int d = nxt <= ncoo ? list[nxt].cs - q0 : 32;
+          const unsigned mask = __reduce_or_sync(0xffffffffu, (d >= 0 && d < 32) ? 1u << d : 0u);
+          int blk = ia + __popc(mask & ((2u << lane) - 1u));
+          blk = min(blk, ncoo - 1);
+          const int q = q0 + lane;
+          HCooRaw<V>& r = raw[u];
+          r.ok = q < ntot;
+          if (r.ok) {
+            const HBlk h = list[blk];
+            const int e = q - h.cs;
+            const int64_t k = (int64_t)h.bp + e;
+            r.row = ld_stream(row_ptr + h.off + e, pf);
+            r.col = (uint32_t)ld_stream(col_idx + k, pf);
+            r.v = ld_stream(values + k, pf);
+            r.xoff = (int64_t)h.j * C;
+          }
+          ia = __shfl_sync(0xffffffffu, blk, 31);
+        }
+      };
+      coo_load(0);
+      for (int t = 0; t < nrounds; ++t) {
+        // products of this round into shared memory, in stream order
+#pragma unroll
+        for (int u = 0; u < kHU; ++u) {
+          const int i = warp * (kHU * 32) + 32 * u + lane;
+          const HCooRaw<V>& r = raw[u];
+          P pv = P(0);
+          uint32_t own = 0xFFu;
+          if (r.ok) {
+            const X xv = ld_keep(x + r.xoff + r.col, pl);
+            if constexpr (MIX) pv = to_f32(r.v) * (float)xv;
+            else pv = (P)(r.v * xv);
+            own = (uint32_t)(((int64_t)kHW * r.row) / rows);
+          }
+          s_prod[i] = pv;
+          s_row[i] = r.ok ? r.row : 0u;
+          s_own[i] = (uint8_t)own;
+        }
+        __syncthreads();
+        if (t + 1 < nrounds) coo_load(t + 1);
+        // this warp's nonzeros of the round, in stream order
+        const uint32_t me = (uint32_t)warp * 0x01010101u;
+#pragma unroll 1
+        for (int it = 0; it < kHRound / 512; ++it) {
+          const uint4 w4 = reinterpret_cast<const uint4*>(s_own)[it * 32 + lane];
+          const uint32_t ws[4] = {w4.x, w4.y, w4.z, w4.w};
+          uint32_t m16 = 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t eq = __vcmpeq4(ws[q], me);
+            m16 |= (((eq >> 7) & 1u) | ((eq >> 14) & 2u) | ((eq >> 21) & 4u) | ((eq >> 28) & 8u)) << (4 * q);
+          }
+          const int cnt = __popc(m16);
+          int inc = cnt;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, inc, d);
+            if (lane >= d) inc += o;
+          }
+          const int total = __shfl_sync(0xffffffffu, inc, 31);
+          int pos = inc - cnt;
+          while (m16) {
+            const int b = __ffs(m16) - 1;
+            olist[pos++] = (uint16_t)(it * 512 + 16 * lane + b);
+            m16 &= m16 - 1u;
+          }
+          __syncwarp();
+          for (int g = 0; g < total; g += 32) {
+            const int tt = g + lane;
+            uint32_t r = 0xFFFFFFFFu;
+            SA pv = SA(0);
+            if (tt < total) {
+              const int i = olist[tt];
+              r = s_row[i];
+              pv = (SA)s_prod[i];
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, r);
+            const int np = __popc(peers);
+            const int maxnp = (int)__reduce_max_sync(0xffffffffu, (unsigned)np);
+            SA s = pv;
+            for (int k = 1; k < maxnp; ++k) {  // the row's other values, in lane order
+              const int src = k < np ? (int)__fns(peers, 0, k + 1) : lane;
+              const SA ov = __shfl_sync(0xffffffffu, pv, src);
+              if (k < np) s += ov;
+            }
+            if (tt < total && lane == __ffs(peers) - 1) acc[r] += s;
+            __syncwarp();
+          }
+        }
+        __syncthreads();
+      }
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  for (int li = tid; li < rows; li += kHT) {
+    const X o = (X)acc[li];
+    X* yp = y + r0 + li;
+    *yp = (beta == X(0)) ? alpha * o : alpha * o + beta * *yp;
+  }
+}
+
+int hcsr_validate(const rvvla_hcsr* A, const void* x, const void* y) {
+  if (!A) return fail(RVVLA_ERR_INVALID_ARG, "hcsr: null descriptor");
+  if (A->R <= 0 || A->C <= 0 || A->m < 0 || A->n < 0 || A->nz < 0)
+    return fail(RVVLA_ERR_INVALID_ARG, "hcsr: bad sizes");
+  if (A->b_m != (A->m + A->R - 1) / A->R || A->b_n != (A->n + A->C - 1) / A->C)
+    return fail(RVVLA_ERR_FORMAT, "hcsr: b_m/b_n inconsistent with m, n, R, C");
+  if (A->m > 0 && (!A->block_ptr || !A->row_offset || !y)) return fail(RVVLA_ERR_INVALID_ARG, "hcsr: null array");
+  if (A->nz > 0 && (!A->col_idx || !A->values || !A->row_ptr || !x))
+    return fail(RVVLA_ERR_INVALID_ARG, "hcsr: null array");
+  if (A->C > 65536) return fail(RVVLA_ERR_TOO_LARGE, "hcsr: C > 65536 does not fit the uint16 col_idx");
+  if (A->m > INT32_MAX || A->nz > INT32_MAX) return fail(RVVLA_ERR_TOO_LARGE, "hcsr: m or nz beyond 2^31 - 1");
+  return RVVLA_OK;
+}
+
+// Largest dynamic shared memory one CTA may take (227 KB on sm_100a).
+constexpr size_t kHSmemMax = 227 * 1024;
+
+template <class V, class X, class SA, bool MIX, bool VEC, bool GACC>
+int hcsr_launch(const rvvla_hcsr* A, X alpha, const X* x, X beta, X* y, SA* gacc, size_t smem, cudaStream_t st) {
+  auto kern = hcsr_spmv_kernel<V, X, SA, MIX, VEC, GACC>;
+  RVVLA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  prefer_shared(kern);
+  kern<<<(unsigned)A->b_m, kHT, smem, st>>>(A->R, A->C, A->m, A->nz, A->b_n, A->block_ptr, A->row_offset,
+                                            A->row_ptr, A->col_idx, (const V*)A->values, x, y, alpha, beta, gacc);
+  RVVLA_LAUNCHED("hcsr_spmv_kernel");
+  return RVVLA_OK;
+}
+
+template <class V, class X, class SA, bool MIX>
+int hcsr_spmv_impl(const rvvla_hcsr* A, X alpha, const X* x, X beta, X* y, cudaStream_t st) {
+  using P = typename HTypes<V, X, SA, MIX>::P;
+  int rc = hcsr_validate(A, x, y);
+  if (rc) return rc;
+  if (A->m == 0) return RVVLA_OK;
+  if (A->b_m > INT32_MAX) return fail(RVVLA_ERR_TOO_LARGE, "hcsr: more than 2^31 - 1 block rows");
+  const bool vec = ((uintptr_t)A->values % 16 == 0) && ((uintptr_t)A->col_idx % 16 == 0);
+  const int64_t racc = std::min<int64_t>(A->R, A->m);
+  const size_t smem_s = HLayout<SA, P>(racc).total;
+  if (smem_s <= kHSmemMax) {
+    return vec ? hcsr_launch<V, X, SA, MIX, true, false>(A, alpha, x, beta, y, nullptr, smem_s, st)
+               : hcsr_launch<V, X, SA, MIX, false, false>(A, alpha, x, beta, y, nullptr, smem_s, st);
+  }
+  // block rows too tall for shared memory: the accumulator is a global
+  // scratch array (each CTA owns its slice)
+  Scratch sc;
+  RVVLA_CUDA(sc.alloc((size_t)A->m * sizeof(SA), st));
+  const size_t smem_g = HLayout<SA, P>(0).total;
+  return vec ? hcsr_launch<V, X, SA, MIX, true, true>(A, alpha, x, beta, y, sc.as<SA>(), smem_g, st)
+             : hcsr_launch<V, X, SA, MIX, false, true>(A, alpha, x, beta, y, sc.as<SA>(), smem_g, st);
+}
+
+}  // namespace
+}  // namespace rvvla
+
+using namespace rvvla;
+
+extern "C" {
+
+int rvvla_hcsr_spmv_f64(const rvvla_hcsr* A, double alpha, const double* x, double beta, double* y, void* stream) {
+  return hcsr_spmv_impl<double, double, double, false>(A, alpha, x, beta, y, as_stream(stream));
+}
+
+int rvvla_hcsr_spmv_f32(const rvvla_hcsr* A, float alpha, const float* x, float beta, float* y, void* stream) {
+  return hcsr_spmv_impl<float, float, float, false>(A, alpha, x, beta, y, as_stream(stream));
+}
+
+int rvvla_hcsr_spmv_mixed(const rvvla_hcsr* A, int val_type, float alpha, const float* x, float beta, float* y,
+                          void* stream) {
+  if (val_type == RVVLA_F32)
+    return hcsr_spmv_impl<float, float, double, true>(A, alpha, x, beta, y, as_stream(stream));
+  if (val_type == RVVLA_BF16)
+    return hcsr_spmv_impl<__nv_bfloat16, float, double, true>(A, alpha, x, beta, y, as_stream(stream));
+  return fail(RVVLA_ERR_INVALID_ARG, "hcsr_spmv_mixed: val_type must be RVVLA_F32 or RVVLA_BF16");
+}
+
+}  // extern "C"
