@@ -77,12 +77,57 @@ def _lib():
             "orc_crs_spmv_ld": (None, [vp, dbl, vp, dbl, vp]),
             "orc_sddmm": (None, [vp, vp, vp, vp]),
             "orc_merge_path": (None, [i64, vp, i64, i64, vp]),
+            # the seeded workload generators (the library's gen.cpp)
+            "rvvla_gen_laplace2d": (i64, [i64, vp, vp, vp]),
+            "rvvla_gen_stencil27": (i64, [i64, C.c_uint64, vp, vp, vp]),
+            "rvvla_gen_powerlaw": (i64, [i64, dbl, dbl, i64, i64, dbl, C.c_uint64, vp, vp, vp]),
+            "rvvla_gen_random_rows": (i64, [i64, i64, cint, dbl, cint, C.c_uint64, vp, vp, vp]),
+            "rvvla_gen_vector": (None, [i64, C.c_uint64, cint, dbl, dbl, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
         _olib = L
     return _olib
+
+
+# ------------------------------------------------------------ workloads
+# The same seeded generators the CUDA library exports (gen.cpp is compiled
+# into both), for callers that must not load the CUDA library: the bench's
+# CPU-only reference arm.  tests/test_bench_reference_arm.py checks that both
+# give equal bits.
+def _gen_two_pass(name, m, *args):
+    fn = getattr(_lib(), "rvvla_gen_" + name)
+    nz = int(fn(*args, None, None, None))
+    if nz < 0:
+        raise ValueError("generator rejected its arguments")
+    Rst = np.empty(m + 1, dtype=np.int32)
+    Col = np.empty(nz, dtype=np.int32)
+    Val = np.empty(nz, dtype=np.float64)
+    fn(*args, Rst.ctypes.data, Col.ctypes.data, Val.ctypes.data)
+    return Rst, Col, Val
+
+
+def gen_laplace2d(g: int):
+    Rst, Col, Val = _gen_two_pass("laplace2d", g * g, g)
+    return g * g, g * g, Rst, Col, Val
+
+
+def gen_stencil27(g: int, seed: int = 3):
+    Rst, Col, Val = _gen_two_pass("stencil27", g ** 3, g, seed)
+    return g ** 3, g ** 3, Rst, Col, Val
+
+
+def gen_powerlaw(n: int, mean: float = 16.0, sigma: float = 1.2, cap: int = 4096, band: int = 1024,
+                 band_frac: float = 0.7, seed: int = 1):
+    Rst, Col, Val = _gen_two_pass("powerlaw", n, n, mean, sigma, cap, band, band_frac, seed)
+    return n, n, Rst, Col, Val
+
+
+def gen_vector(n: int, seed: int = 0, normal: bool = False, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
+    out = np.empty(n, dtype=np.float64)
+    _lib().rvvla_gen_vector(n, seed, 1 if normal else 0, lo, hi, out.ctypes.data)
+    return out
 
 
 class Bundle:
