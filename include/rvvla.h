@@ -82,6 +82,16 @@ int rvvla_memcpy(void* dst, const void* src, size_t bytes, void* stream);
  * rvvla_malloc of 0 bytes yields NULL. */
 int rvvla_malloc(void** ptr, size_t bytes);
 int rvvla_free(void* ptr);
+/* Copies from pageable host memory to the device (no reference counterpart:
+ * the reference's vectors never leave the host).  Large copies go through
+ * the library's page-locked staging buffers in 4 MB chunks, the host memcpy
+ * of one chunk (several threads) overlapping the DMA of the previous one.
+ * Returns once `src` may be reused; the transfer is ordered on `stream`
+ * before later work there. */
+int rvvla_copy_h2d(void* dst, const void* src, size_t bytes, void* stream);
+/* Device to pageable host memory through the same staging; ordered after
+ * earlier work on `stream`, returns once `dst` holds the data. */
+int rvvla_copy_d2h(void* dst, const void* src, size_t bytes, void* stream);
 /* Synchronises `stream`, then reads and clears the device status word that
  * kernels with bounded waits (the bulk-copy pipelines) set when a wait
  * expires.  *code = 0 and RVVLA_OK when no wait expired since the last call;

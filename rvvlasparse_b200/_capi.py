@@ -186,6 +186,8 @@ def load():
     _proto(lib, "rvvla_device_info", cint, P(cint), P(cint), P(cint))
     _proto(lib, "rvvla_kernel_launch_count", u64)
     _proto(lib, "rvvla_memcpy", cint, vp, vp, C.c_size_t, vp)
+    _proto(lib, "rvvla_copy_h2d", cint, vp, vp, C.c_size_t, vp)
+    _proto(lib, "rvvla_copy_d2h", cint, vp, vp, C.c_size_t, vp)
     _proto(lib, "rvvla_malloc", cint, P(vp), C.c_size_t)
     _proto(lib, "rvvla_free", cint, vp)
     _proto(lib, "rvvla_device_status", cint, P(cint), vp)

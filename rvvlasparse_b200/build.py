@@ -107,11 +107,13 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
 DROPIN = os.path.join(PKG, "dropin")
 DROPIN_LIB = os.path.join(LIB_DIR, "librvvla_dropin.so")
 DROPIN_TEST = os.path.join(PKG, "_build", "test_dropin")
+DROPIN_BENCH = os.path.join(PKG, "_build", "bench_dropin")
 
 
 def build_dropin(verbose: bool = False) -> str:
-    """Compile the C++ drop-in library and its test program (host code only,
-    linked against ``librvvla_b200.so``); returns the library path."""
+    """Compile the C++ drop-in library, its test program and the bench's
+    end-to-end harness (host code only, linked against ``librvvla_b200.so``);
+    returns the library path."""
     cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
     inc = ["-I" + INCLUDE, "-I" + os.path.join(DROPIN, "include")]
     hdrs = glob.glob(os.path.join(DROPIN, "include", "*.h")) + [os.path.join(INCLUDE, "rvvla.h")]
@@ -121,6 +123,9 @@ def build_dropin(verbose: bool = False) -> str:
           "-L" + LIB_DIR, "-lrvvla_b200", "-Wl,-rpath,$ORIGIN", "-o"]),
         (DROPIN_TEST, [os.path.join(DROPIN, "test_dropin.cpp"), DROPIN_LIB],
          [cxx, "-std=c++17", "-O2", "-Wall"] + inc + [os.path.join(DROPIN, "test_dropin.cpp"), "-L" + LIB_DIR,
+          "-lrvvla_dropin", "-lrvvla_b200", "-Wl,-rpath,$ORIGIN/../lib", "-o"]),
+        (DROPIN_BENCH, [os.path.join(DROPIN, "bench_dropin.cpp"), DROPIN_LIB],
+         [cxx, "-std=c++17", "-O2", "-Wall"] + inc + [os.path.join(DROPIN, "bench_dropin.cpp"), "-L" + LIB_DIR,
           "-lrvvla_dropin", "-lrvvla_b200", "-Wl,-rpath,$ORIGIN/../lib", "-o"]),
     ]
     os.makedirs(os.path.dirname(DROPIN_TEST), exist_ok=True)

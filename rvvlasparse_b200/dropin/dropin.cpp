@@ -173,10 +173,12 @@ sparse_matrix_status run(DeviceMirror& M, size_t m, size_t n, const std::vector<
   }
   ensure(M.x, M.xbytes, std::max<size_t>(n, 1) * sizeof(T));
   ensure(M.y, M.ybytes, std::max<size_t>(m, 1) * sizeof(T));
-  if (n) check(rvvla_memcpy(M.x, b.data(), n * sizeof(T), nullptr), "rvvla_memcpy");
-  if (m && (reads_y || beta != T(0))) check(rvvla_memcpy(M.y, y.data(), m * sizeof(T), nullptr), "rvvla_memcpy");
+  // the caller's vectors are pageable: staged through the library's
+  // page-locked buffers, host copies overlapping the DMA
+  if (n) check(rvvla_copy_h2d(M.x, b.data(), n * sizeof(T), nullptr), "rvvla_copy_h2d");
+  if (m && (reads_y || beta != T(0))) check(rvvla_copy_h2d(M.y, y.data(), m * sizeof(T), nullptr), "rvvla_copy_h2d");
   st.code = call(static_cast<const T*>(M.x), static_cast<T*>(M.y));
-  if (st.code == RVVLA_OK && m) check(rvvla_memcpy(y.data(), M.y, m * sizeof(T), nullptr), "rvvla_memcpy");
+  if (st.code == RVVLA_OK && m) check(rvvla_copy_d2h(y.data(), M.y, m * sizeof(T), nullptr), "rvvla_copy_d2h");
   return st;
 }
 
@@ -717,6 +719,39 @@ sparse_matrix_status sell_spmv(sparse_operation_t op, T alpha, const spMtxSELL_C
 }
 RVVLA_DROPIN_SPMV(spMtxSELL_C_Sigma, double, { return sell_spmv<double>(op, alpha, A, b, beta, y, stage); })
 RVVLA_DROPIN_SPMV(spMtxSELL_C_Sigma, float, { return sell_spmv<float>(op, alpha, A, b, beta, y, stage); })
+
+// ------------------------------------------------------------------ mixed precision
+#define RVVLA_DROPIN_MIXED(CLS, MIRROR, FIELD, FN, ROWS, COLS)                                                \
+  sparse_matrix_status rvvla_sparse_mv_mixed(sparse_operation_t op, float alpha, const CLS<float>& A,          \
+                                             const std::vector<float>& b, float beta, std::vector<float>& y) { \
+    if (op != SPARSE_OPERATION_NON_TRANSPOSE) return unsupported_op<float>();                                 \
+    return guarded([&] {                                                                                       \
+      DeviceMirror& M = MIRROR(A);                                                                             \
+      return run<float>(M, (size_t)(ROWS), (size_t)(COLS), b, beta, y, false, [&](const float* x, float* yy) { \
+        return FN(&M.FIELD, RVVLA_F32, alpha, x, beta, yy, nullptr);                                           \
+      });                                                                                                      \
+    });                                                                                                        \
+  }
+
+RVVLA_DROPIN_MIXED(spMtxCRS, crs_mirror, crs, rvvla_crs_spmv_mixed, A.m, A.n)
+RVVLA_DROPIN_MIXED(spMtxHCSR, hcsr_mirror, hcsr, rvvla_hcsr_spmv_mixed, A.m, A.n)
+RVVLA_DROPIN_MIXED(spMtxSELL_C_Sigma, sell_mirror, sell, rvvla_sell_spmv_mixed, A.m, A.n)
+
+sparse_matrix_status rvvla_sparse_mv_mixed(sparse_operation_t op, float alpha, const spMtxCSR5<float>& A,
+                                           const std::vector<float>& b, float beta, std::vector<float>& y) {
+  if (op != SPARSE_OPERATION_NON_TRANSPOSE) return unsupported_op<float>();
+  if (A.format() != CSR5_FORMAT_CSR5) {
+    sparse_matrix_status st;
+    st.code = RVVLA_ERR_FORMAT;
+    return st;
+  }
+  return guarded([&] {
+    DeviceMirror& M = csr5_mirror(A);
+    return run<float>(M, (size_t)A._m, (size_t)A._n, b, beta, y, false, [&](const float* x, float* yy) {
+      return rvvla_csr5_spmv_mixed(&M.csr5, RVVLA_F32, alpha, x, beta, yy, nullptr);
+    });
+  });
+}
 
 #define RVVLA_DROPIN_CONVERT(CLS, FN)                                                                        \
   void rvvla_convert(CLS<double>& dist, const spMtxCRS<double>& src, const convertParams& p) { FN(dist, src, p); } \

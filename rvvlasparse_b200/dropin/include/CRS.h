@@ -172,5 +172,6 @@ class spMtxCRS {
 };
 
 RVVLA_DROPIN_DECLARE_SPMV(spMtxCRS)
+RVVLA_DROPIN_DECLARE_SPMV_MIXED(spMtxCRS)
 
 }  // namespace SparseMatrixLib

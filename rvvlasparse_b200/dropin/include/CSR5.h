@@ -96,6 +96,7 @@ class spMtxCSR5 {
 };
 
 RVVLA_DROPIN_DECLARE_SPMV(spMtxCSR5)
+RVVLA_DROPIN_DECLARE_SPMV_MIXED(spMtxCSR5)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxCSR5)
 
 }  // namespace SparseMatrixLib

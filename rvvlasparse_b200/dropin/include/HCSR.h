@@ -46,6 +46,7 @@ class spMtxHCSR {
 };
 
 RVVLA_DROPIN_DECLARE_SPMV(spMtxHCSR)
+RVVLA_DROPIN_DECLARE_SPMV_MIXED(spMtxHCSR)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxHCSR)
 
 }  // namespace SparseMatrixLib

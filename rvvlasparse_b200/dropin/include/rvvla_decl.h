@@ -17,3 +17,9 @@
 #define RVVLA_DROPIN_DECLARE_CONVERT(CLS)                                                    \
   void rvvla_convert(CLS<double>& dist, const spMtxCRS<double>& src, const convertParams& p); \
   void rvvla_convert(CLS<float>& dist, const spMtxCRS<float>& src, const convertParams& p);
+
+// the mixed-precision extension (CRS, HCSR, CSR5, SELL-C-sigma): fp32 values,
+// b and y; compensated fp32 sums, fp64 carry merges
+#define RVVLA_DROPIN_DECLARE_SPMV_MIXED(CLS)                                                               \
+  sparse_matrix_status rvvla_sparse_mv_mixed(sparse_operation_t op, float alpha, const CLS<float>& A,     \
+                                             const std::vector<float>& b, float beta, std::vector<float>& y);

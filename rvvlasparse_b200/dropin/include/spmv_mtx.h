@@ -21,4 +21,19 @@ sparse_matrix_status sparse_mv(sparse_operation_t type_op, T alpha, const Mtx<T>
   return rvvla_sparse_mv(type_op, alpha, mat, b, beta, y, stage);  // argument-dependent lookup
 }
 
+// Mixed precision (an addition; the reference has no counterpart): the
+// product of a float matrix (fp32 values) with fp32 b and y whose row sums run
+// in compensated fp32 (two-sum) and whose partial sums of different tiles or
+// blocks merge in fp64 — normwise error ~1e-8 against an fp64 product of the
+// same values, where the plain fp32 product gives ~1e-6.  For spMtxCRS,
+// spMtxHCSR, spMtxCSR5 and spMtxSELL_C_Sigma (all stages at once); op must
+// be SPARSE_OPERATION_NON_TRANSPOSE.
+template <template <class> class Mtx>
+sparse_matrix_status sparse_mv_mixed(sparse_operation_t type_op, float alpha, const Mtx<float>& mat,
+                                     sparse_matrix_descr descr, const std::vector<float>& b, float beta,
+                                     std::vector<float>& y) {
+  (void)descr;
+  return rvvla_sparse_mv_mixed(type_op, alpha, mat, b, beta, y);  // argument-dependent lookup
+}
+
 }  // namespace SparseMatrixLib

@@ -13,6 +13,7 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "sparse_matrix.h"
@@ -118,9 +119,25 @@ void product(const char* fmt, const std::string& tag, const spMtxCRS<T>& A, cons
   }
 }
 
+// the mixed-precision extension on a float matrix: error against the exact
+// product of the same float values within 1e-6
+template <template <class> class Mtx>
+void product_mixed(const char* fmt, const std::string& tag, const spMtxCRS<float>& A, const Mtx<float>& M) {
+  const std::vector<float> b = vec<float>(A.n, 11), y0 = vec<float>(A.m, 12);
+  for (double beta : {0.0, 0.75}) {
+    std::vector<float> y = y0;
+    const sparse_matrix_status st =
+        sparse_mv_mixed<Mtx>(SPARSE_OPERATION_NON_TRANSPOSE, 1.25f, M, sparse_matrix_descr{}, b, (float)beta, y);
+    const double e = relerr(y, host_spmv(A, false, 1.25, b, beta, y0));
+    expect(st.code == 0 && e < 1e-6, std::string(fmt) + " mixed " + tag + " beta=" + std::to_string(beta) +
+                                         " code=" + std::to_string(st.code) + " err=" + std::to_string(e));
+  }
+}
+
 template <class T>
 void run_all(const std::string& tag, const spMtxCRS<T>& A, double tol) {
   product<T, spMtxCRS>("CRS", tag, A, A, tol);
+  if constexpr (std::is_same<T, float>::value) product_mixed<spMtxCRS>("CRS", tag, A, A);
   {  // y = A^T b through the transposed CRS
     const std::vector<T> b = vec<T>(A.m, 7), y0 = vec<T>(A.n, 8);
     std::vector<T> y = y0;
@@ -137,6 +154,7 @@ void run_all(const std::string& tag, const spMtxCRS<T>& A, double tol) {
     convert<T, spMtxHCSR>(H, A, p);
     expect(H.values.size() == A.nz && H.block_ptr.back() == (int)A.nz, "HCSR arrays " + tag);
     product<T, spMtxHCSR>("HCSR", tag, A, H, tol);
+    if constexpr (std::is_same<T, float>::value) product_mixed<spMtxHCSR>("HCSR", tag, A, H);
   }
   {
     spMtxSELL_C_Sigma<T> S;
@@ -145,6 +163,7 @@ void run_all(const std::string& tag, const spMtxCRS<T>& A, double tol) {
     p.param["Sigma"].i = 128;
     convert<T, spMtxSELL_C_Sigma>(S, A, p);
     product<T, spMtxSELL_C_Sigma>("SELL", tag, A, S, tol);
+    if constexpr (std::is_same<T, float>::value) product_mixed<spMtxSELL_C_Sigma>("SELL", tag, A, S);
     // the three stages one after another equal ALL_STAGES
     const std::vector<T> b = vec<T>(A.n, 9), y0 = vec<T>(A.m, 10);
     std::vector<T> y = y0;
@@ -164,6 +183,7 @@ void run_all(const std::string& tag, const spMtxCRS<T>& A, double tol) {
     convert<T, spMtxCSR5>(C5, A, p);
     expect(C5._omega == 32 && C5._csr_value.size() == A.nz, "CSR5 fields " + tag);
     product<T, spMtxCSR5>("CSR5", tag, A, C5, tol);
+    if constexpr (std::is_same<T, float>::value) product_mixed<spMtxCSR5>("CSR5", tag, A, C5);
     spMtxCSR5<T> D;  // the reference's member-function route
     D.inputCSR((int)A.m, (int)A.n, (int)A.nz, A.Rst, A.Col, A.Val);
     expect(D.asCSR5(p) == CSR5_SUCCESS, "CSR5 asCSR5 " + tag);
