@@ -594,6 +594,45 @@ int rvvla_batched_graph(const rvvla_batch* B, double alpha, const void* X, doubl
                         void* stream, void** graph);
 int rvvla_batched_graph_launch(void* graph, void* stream);
 void rvvla_batched_graph_free(void* graph);
+/* ------------------------------------------------------------ autotuner
+ * Parameters for convert (the reference's convertParams bag,
+ * include/convert.h:21-28, whose keys the drop-in fills from these fields):
+ * HCSR "R", "C", "p"; SELL "C", "Sigma"; CSR5 "sigma" (omega 32); LAV
+ * "SIMD_Lanes", "T", "segment_len"; VHCC "num_threads"; CVR "Nthreads". */
+typedef enum rvvla_format {
+  RVVLA_FMT_HCSR = 1,
+  RVVLA_FMT_SELL = 2,
+  RVVLA_FMT_CSR5 = 3,
+  RVVLA_FMT_LAV = 4,
+  RVVLA_FMT_VHCC = 5,
+  RVVLA_FMT_CVR = 6
+} rvvla_format;
+
+typedef struct rvvla_tune_params {
+  int64_t R, C;                     /* HCSR block rows/columns; SELL slice height in C */
+  double p;                         /* HCSR CSR/COO threshold */
+  int64_t sigma;                    /* SELL-C-sigma window; CSR5 sigma */
+  int64_t threads;                  /* VHCC num_threads; CVR Nthreads */
+  int64_t simd_lanes, segment_len;  /* LAV */
+  double T;                         /* LAV dense threshold */
+} rvvla_tune_params;
+
+/* Measuring autotuner for one format (no reference counterpart; the
+ * reference takes its parameters from the caller).  Builds the format on the
+ * GPU from src (values of val_type: RVVLA_F64 / RVVLA_F32, or RVVLA_BF16 with
+ * mixed) for each candidate, times the product (plain, or the mixed form
+ * when mixed != 0: HCSR, SELL, CSR5) with CUDA events, best of iters after
+ * one untimed call, and writes the fastest candidate to *best (and its ms to
+ * *best_ms).  table/table_ms (table_cap entries, may be NULL) receive every
+ * candidate and its time; *n_candidates the count.  Candidates: HCSR R = C in
+ * {512, 1024, 2000, 4000, 8192}, p 2; SELL C 32, sigma {32, 256, 1024, 8192};
+ * CSR5 sigma {8, 16, 24, 32}; LAV segment_len {40000, n/4, n}; VHCC
+ * nnz / {4096, 2048, 1024} threads; CVR nnz / {8192, 32768, 131072} ranges.
+ * Synchronises `stream`. */
+int rvvla_autotune(int format, const rvvla_crs* src, int val_type, int mixed, int iters,
+                   rvvla_tune_params* best, double* best_ms, rvvla_tune_params* table, double* table_ms,
+                   int table_cap, int* n_candidates, void* stream);
+
 /* Autotuner: groups the matrices by average row length (powers of two),
  * times every candidate configuration on each group with CUDA events (CSR
  * with 1..32 threads per row for k = 1 or k lanes per row otherwise;

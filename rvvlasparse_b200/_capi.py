@@ -160,6 +160,14 @@ class rvvla_hcsr_owned(C.Structure):
                 ("values", vp)]
 
 
+RVVLA_FMT_HCSR, RVVLA_FMT_SELL, RVVLA_FMT_CSR5, RVVLA_FMT_LAV, RVVLA_FMT_VHCC, RVVLA_FMT_CVR = 1, 2, 3, 4, 5, 6
+
+
+class rvvla_tune_params(C.Structure):
+    _fields_ = [("R", i64), ("C", i64), ("p", C.c_double), ("sigma", i64), ("threads", i64), ("simd_lanes", i64),
+                ("segment_len", i64), ("T", C.c_double)]
+
+
 _lib = None
 
 
@@ -187,6 +195,8 @@ def load():
     _proto(lib, "rvvla_kernel_launch_count", u64)
     _proto(lib, "rvvla_memcpy", cint, vp, vp, C.c_size_t, vp)
     _proto(lib, "rvvla_copy_h2d", cint, vp, vp, C.c_size_t, vp)
+    _proto(lib, "rvvla_autotune", cint, cint, P(rvvla_crs), cint, cint, cint, P(rvvla_tune_params),
+           P(C.c_double), P(rvvla_tune_params), P(C.c_double), cint, P(cint), vp)
     _proto(lib, "rvvla_copy_d2h", cint, vp, vp, C.c_size_t, vp)
     _proto(lib, "rvvla_malloc", cint, P(vp), C.c_size_t)
     _proto(lib, "rvvla_free", cint, vp)

@@ -771,4 +771,63 @@ RVVLA_DROPIN_CONVERT(spMtxLAV, lav_convert)
 RVVLA_DROPIN_CONVERT(spMtxVHCC, vhcc_convert)
 RVVLA_DROPIN_CONVERT(spMtxCVR, cvr_convert)
 
+// ------------------------------------------------------------------ autotuner
+namespace {
+
+template <class T>
+convertParams tune(int fmt, const spMtxCRS<T>& src, bool mixed, int iters) {
+  DeviceMirror& S = crs_mirror(src);
+  rvvla_tune_params best{};
+  double ms = 0.0;
+  const int vt = std::is_same<T, double>::value ? RVVLA_F64 : RVVLA_F32;
+  const int rc = rvvla_autotune(fmt, &S.crs, vt, mixed ? 1 : 0, iters, &best, &ms, nullptr, nullptr, 0, nullptr,
+                                nullptr);
+  if (rc) throw_build(rc, "autotune");
+  convertParams p;
+  switch (fmt) {
+    case RVVLA_FMT_HCSR:
+      p.param["R"].i = (int)best.R;
+      p.param["C"].i = (int)best.C;
+      p.param["p"].d = best.p;
+      break;
+    case RVVLA_FMT_SELL:
+      p.param["C"].i = (int)best.C;
+      p.param["Sigma"].i = (int)best.sigma;
+      break;
+    case RVVLA_FMT_CSR5:
+      p.param["omega"].i = 32;
+      p.param["sigma"].i = (int)best.sigma;
+      break;
+    case RVVLA_FMT_LAV:
+      p.param["SIMD_Lanes"].i = (int)best.simd_lanes;
+      p.param["T"].d = best.T;
+      p.param["segment_len"].i = (int)best.segment_len;
+      break;
+    case RVVLA_FMT_VHCC:
+      p.param["num_threads"].i = (int)best.threads;
+      break;
+    default:
+      p.param["Nthreads"].i = (int)best.threads;
+      break;
+  }
+  return p;
+}
+
+}  // namespace
+
+#define RVVLA_DROPIN_TUNE(CLS, FMT)                                                                          \
+  convertParams rvvla_autotune_for(const CLS<double>*, const spMtxCRS<double>& src, bool mixed, int iters) { \
+    return tune<double>(FMT, src, mixed, iters);                                                              \
+  }                                                                                                           \
+  convertParams rvvla_autotune_for(const CLS<float>*, const spMtxCRS<float>& src, bool mixed, int iters) {   \
+    return tune<float>(FMT, src, mixed, iters);                                                               \
+  }
+
+RVVLA_DROPIN_TUNE(spMtxHCSR, RVVLA_FMT_HCSR)
+RVVLA_DROPIN_TUNE(spMtxSELL_C_Sigma, RVVLA_FMT_SELL)
+RVVLA_DROPIN_TUNE(spMtxCSR5, RVVLA_FMT_CSR5)
+RVVLA_DROPIN_TUNE(spMtxLAV, RVVLA_FMT_LAV)
+RVVLA_DROPIN_TUNE(spMtxVHCC, RVVLA_FMT_VHCC)
+RVVLA_DROPIN_TUNE(spMtxCVR, RVVLA_FMT_CVR)
+
 }  // namespace SparseMatrixLib

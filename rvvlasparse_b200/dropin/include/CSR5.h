@@ -98,5 +98,6 @@ class spMtxCSR5 {
 RVVLA_DROPIN_DECLARE_SPMV(spMtxCSR5)
 RVVLA_DROPIN_DECLARE_SPMV_MIXED(spMtxCSR5)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxCSR5)
+RVVLA_DROPIN_DECLARE_TUNE(spMtxCSR5)
 
 }  // namespace SparseMatrixLib

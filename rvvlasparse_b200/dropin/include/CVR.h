@@ -40,5 +40,6 @@ class spMtxCVR {
 
 RVVLA_DROPIN_DECLARE_SPMV(spMtxCVR)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxCVR)
+RVVLA_DROPIN_DECLARE_TUNE(spMtxCVR)
 
 }  // namespace SparseMatrixLib

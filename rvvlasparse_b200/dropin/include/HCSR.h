@@ -48,5 +48,6 @@ class spMtxHCSR {
 RVVLA_DROPIN_DECLARE_SPMV(spMtxHCSR)
 RVVLA_DROPIN_DECLARE_SPMV_MIXED(spMtxHCSR)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxHCSR)
+RVVLA_DROPIN_DECLARE_TUNE(spMtxHCSR)
 
 }  // namespace SparseMatrixLib

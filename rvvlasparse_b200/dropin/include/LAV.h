@@ -48,5 +48,6 @@ struct spMtxLAV {
 
 RVVLA_DROPIN_DECLARE_SPMV(spMtxLAV)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxLAV)
+RVVLA_DROPIN_DECLARE_TUNE(spMtxLAV)
 
 }  // namespace SparseMatrixLib

@@ -38,5 +38,6 @@ class spMtxSELL_C_Sigma {
 RVVLA_DROPIN_DECLARE_SPMV(spMtxSELL_C_Sigma)
 RVVLA_DROPIN_DECLARE_SPMV_MIXED(spMtxSELL_C_Sigma)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxSELL_C_Sigma)
+RVVLA_DROPIN_DECLARE_TUNE(spMtxSELL_C_Sigma)
 
 }  // namespace SparseMatrixLib

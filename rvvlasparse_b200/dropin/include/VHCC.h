@@ -102,5 +102,6 @@ class spMtxVHCC {
 
 RVVLA_DROPIN_DECLARE_SPMV(spMtxVHCC)
 RVVLA_DROPIN_DECLARE_CONVERT(spMtxVHCC)
+RVVLA_DROPIN_DECLARE_TUNE(spMtxVHCC)
 
 }  // namespace SparseMatrixLib

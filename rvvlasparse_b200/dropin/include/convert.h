@@ -30,4 +30,18 @@ void convert(MtxDist<T>& dist, const spMtxCRS<T>& src, const convertParams& para
   rvvla_convert(dist, src, params);  // found by argument-dependent lookup
 }
 
+// Measuring autotuner (an addition; the reference takes every parameter from
+// the caller): builds MtxDist from src for each candidate on the GPU, times
+// the product (the mixed-precision one when mixed is set: HCSR, SELL, CSR5
+// with float values) and returns the convertParams of the fastest, ready for
+// convert().  Candidates: HCSR R = C in {512, 1024, 2000, 4000, 8192}, p 2;
+// SELL C 32, Sigma {32, 256, 1024, 8192}; CSR5 sigma {8, 16, 24, 32}; LAV
+// segment_len {40000, n/4, n}; VHCC num_threads and CVR Nthreads from the
+// nonzero count.  Throws like convert on failure.
+template <class T, template <class> class MtxDist>
+convertParams autotune(const spMtxCRS<T>& src, bool mixed = false, int iters = 5) {
+  const MtxDist<T>* tag = nullptr;
+  return rvvla_autotune_for(tag, src, mixed, iters);  // found by argument-dependent lookup
+}
+
 }  // namespace SparseMatrixLib

@@ -23,3 +23,9 @@
 #define RVVLA_DROPIN_DECLARE_SPMV_MIXED(CLS)                                                               \
   sparse_matrix_status rvvla_sparse_mv_mixed(sparse_operation_t op, float alpha, const CLS<float>& A,     \
                                              const std::vector<float>& b, float beta, std::vector<float>& y);
+
+// the measuring autotuner (an addition): convertParams of the fastest
+// candidate for CLS built from src; the pointer argument only selects CLS
+#define RVVLA_DROPIN_DECLARE_TUNE(CLS)                                                                          \
+  convertParams rvvla_autotune_for(const CLS<double>* tag, const spMtxCRS<double>& src, bool mixed, int iters); \
+  convertParams rvvla_autotune_for(const CLS<float>* tag, const spMtxCRS<float>& src, bool mixed, int iters);

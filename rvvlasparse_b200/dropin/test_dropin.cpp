@@ -234,6 +234,21 @@ int main(int argc, char** argv) {
     run_all<float>("laplace64 f32", laplace<float>(64), 1e-5);
     run_all<double>("irregular f64", irregular<double>(5000, 4000, 3), 1e-12);
     run_all<float>("irregular f32", irregular<float>(5000, 4000, 4), 1e-5);
+    {  // the autotuner's parameters build a format that multiplies correctly
+      spMtxCRS<float> A = irregular<float>(20000, 15000, 9);
+      const convertParams ph = autotune<float, spMtxHCSR>(A, true, 2);
+      spMtxHCSR<float> H;
+      convert<float, spMtxHCSR>(H, A, ph);
+      product_mixed<spMtxHCSR>("HCSR(tuned)", "irregular f32", A, H);
+      const convertParams pc = autotune<float, spMtxCSR5>(A, false, 2);
+      spMtxCSR5<float> C5;
+      convert<float, spMtxCSR5>(C5, A, pc);
+      product<float, spMtxCSR5>("CSR5(tuned)", "irregular f32", A, C5, 1e-5);
+      spMtxCRS<double> A64 = irregular<double>(20000, 15000, 10);
+      spMtxSELL_C_Sigma<double> S;
+      convert<double, spMtxSELL_C_Sigma>(S, A64, autotune<double, spMtxSELL_C_Sigma>(A64, false, 2));
+      product<double, spMtxSELL_C_Sigma>("SELL(tuned)", "irregular f64", A64, S, 1e-12);
+    }
     {  // reference error behaviour of the HCSR builder
       spMtxHCSR<double> H;
       convertParams p;

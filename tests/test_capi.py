@@ -89,3 +89,26 @@ def test_random_rows_geometric_mean():
     m, n, R, Cc, V = W.random_rows(100000, 100000, "geometric", 1 / 19, "normal", seed=4)
     ln = np.diff(R)
     assert ln.min() >= 1 and 18.0 < ln.mean() < 20.0
+
+
+def test_autotune_and_host_copies_validate_before_the_gpu():
+    """rvvla_autotune and the staged host copies reject bad arguments
+    without touching a device."""
+    lib = _capi.load()
+    best = _capi.rvvla_tune_params()
+    E = _capi.RVVLA_ERR_INVALID_ARG
+    assert lib.rvvla_autotune(_capi.RVVLA_FMT_HCSR, None, 0, 0, 1, C.byref(best), None, None, None, 0, None,
+                              None) == E
+    d = _capi.rvvla_crs(4, 4, 4, None, None, None, None, 0)
+    # the mixed form needs F32 or BF16 values, and exists for HCSR / SELL / CSR5 only
+    assert lib.rvvla_autotune(_capi.RVVLA_FMT_HCSR, C.byref(d), _capi.RVVLA_F64, 1, 1, C.byref(best), None, None,
+                              None, 0, None, None) == E
+    assert lib.rvvla_autotune(_capi.RVVLA_FMT_CVR, C.byref(d), _capi.RVVLA_F32, 1, 1, C.byref(best), None, None,
+                              None, 0, None, None) == E
+    assert lib.rvvla_autotune(99, C.byref(d), _capi.RVVLA_F64, 0, 1, C.byref(best), None, None, None, 0, None,
+                              None) == E
+    assert lib.rvvla_autotune(_capi.RVVLA_FMT_CSR5, C.byref(d), 7, 0, 1, C.byref(best), None, None, None, 0, None,
+                              None) == E
+    assert lib.rvvla_copy_h2d(None, None, 16, None) == E
+    assert lib.rvvla_copy_d2h(None, None, 16, None) == E
+    assert lib.rvvla_copy_h2d(None, None, 0, None) == _capi.RVVLA_OK
