@@ -1,4 +1,4 @@
-// lav.cu — spMtxLAV on sm_100a: builder (host, then uploaded) and SpMV.
+// lav.cu — spMtxLAV on sm_100a: SpMV (the builder is in lav_build.cu, on the GPU).
 //
 // Layout (include/LAV.h:10-31 of the reference) as read by
 // src/scalar/spmv_mtx_lav.cpp:36-79: dense columns cut into segments; per
@@ -24,7 +24,6 @@
 #include <vector>
 
 #include "crs_merge.cuh"
-#include "lav_build.h"
 #include "rvvla_internal.cuh"
 
 extern "C" int rvvla_crs_spmv_f64(const rvvla_crs*, double, const double*, double, double*, void*);
@@ -175,54 +174,19 @@ lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, int64_t n, int64_t nlong, 
 
 constexpr int64_t kLavLongSteps = 128;
 
+
 template <class T>
-int upload(const std::vector<T>& v, T** dst, cudaStream_t st) {
-  RVVLA_CUDA(cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)));
-  if (!v.empty()) RVVLA_CUDA(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-  return RVVLA_OK;
-}
+int lav_build_gpu(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen, int64_t long_steps,
+                  rvvla_lav_owned* out, cudaStream_t st);
 
 template <class T>
 int lav_build_typed(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen, rvvla_lav_owned* out, cudaStream_t st) {
-  const int64_t m = src->m, nz = src->nz;
-  std::vector<int> Rst((size_t)m + 1), Col((size_t)nz);
-  std::vector<T> Val((size_t)nz);
-  RVVLA_CUDA(cudaMemcpyAsync(Rst.data(), src->Rst, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
-  if (nz) {
-    RVVLA_CUDA(cudaMemcpyAsync(Col.data(), src->Col, nz * sizeof(int), cudaMemcpyDeviceToHost, st));
-    RVVLA_CUDA(cudaMemcpyAsync(Val.data(), src->Val, nz * sizeof(T), cudaMemcpyDeviceToHost, st));
-  }
-  RVVLA_CUDA(cudaStreamSynchronize(st));
-  LavHost<T> H;
-  lav_build_host<T>(Rst.data(), Col.data(), Val.data(), m, src->n, nz, L, Tthr, seglen, H);
+  if (src->m > 0 && (!src->Rst || (src->nz > 0 && (!src->Col || !src->Val))))
+    return fail(RVVLA_ERR_INVALID_ARG, "lav_build: null array");
+  int rc = lav_build_gpu<T>(src, L, Tthr, seglen, kLavLongSteps, out, st);
+  if (rc) return rc;
   rvvla_lav& h = out->h;
-  h.SIMD_Lanes = L; h.m = m; h.n = src->n; h.nz = nz; h.segment_count = H.nseg; h.chunk_count = H.cc;
-  h.segment_len = seglen; h.T = Tthr; h.n_steps = (int64_t)H.mk.size();
-  int rc = 0;
-  if ((rc = upload(H.co, &out->chunk_offsets, st)) || (rc = upload(H.cf, &out->chunk_offsets_full_mask, st)) ||
-      (rc = upload(H.sp, &out->segment_ptr, st)) || (rc = upload(H.oo, &out->out_order, st)) ||
-      (rc = upload(H.mk, &out->mask, st)) || (rc = upload(H.val, reinterpret_cast<T**>(&out->val), st)) ||
-      (rc = upload(H.col, &out->col_id, st)) || (rc = upload(H.sRst, &out->sp_Rst, st)) ||
-      (rc = upload(H.sCol, &out->sp_Col, st)) || (rc = upload(H.sVal, reinterpret_cast<T**>(&out->sp_Val), st)) ||
-      (rc = upload(H.row_order, &out->row_order, st)))
-    return rc;
-  if (!H.lane_of_slot.empty() && (rc = upload(H.lane_of_slot, &out->lane_of_slot, st))) return rc;
-  h.chunk_offsets = out->chunk_offsets; h.chunk_offsets_full_mask = out->chunk_offsets_full_mask;
-  h.segment_ptr = out->segment_ptr; h.out_order = out->out_order; h.mask = out->mask; h.val = out->val;
-  h.col_id = out->col_id;
-  h.row_order = out->row_order;
-  h.lane_of_slot = out->lane_of_slot;
-  // the leading chunks up to the last one of >= kLavLongSteps steps (summed
-  // over the segments) get a thread block each
-  h.long_chunks = 0;
-  for (int64_t c = 0; c < H.cc; ++c) {
-    int64_t steps = 0;
-    for (int64_t s = 0; s < H.nseg; ++s) steps += H.co[(size_t)((H.cc + 1) * s + c + 1)] - H.co[(size_t)((H.cc + 1) * s + c)];
-    if (steps >= kLavLongSteps) h.long_chunks = c + 1;
-  }
-  h.sparse_part.m = m; h.sparse_part.n = src->n; h.sparse_part.nz = (int64_t)H.sCol.size();
-  h.sparse_part.Rst = out->sp_Rst; h.sparse_part.Col = out->sp_Col; h.sparse_part.Val = out->sp_Val;
-  h.sparse_part.plan = nullptr; h.sparse_part.plan_tiles = 0; h.sparse_part.plan_kind = 0;
+  const int64_t m = src->m;
   if (h.sparse_part.nz > 0) {  // analyse the sparse part once for the CRS lane-run kernel
     const int dt = sizeof(T) == 8 ? RVVLA_F64 : RVVLA_F32;
     const int64_t plen = rvvla_crs_plan_len(m, h.sparse_part.nz, dt);

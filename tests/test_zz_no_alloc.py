@@ -61,6 +61,12 @@ def _default_pool():
     return rt, pool
 
 
+def _u64(v):
+    from cuda.bindings import driver
+
+    return driver.cuuint64_t(v)
+
+
 def _pool_attr(rt, pool, attr):
     err, v = rt.cudaMemPoolGetAttribute(pool, attr)
     assert err == rt.cudaError_t.cudaSuccess, err
@@ -89,7 +95,7 @@ def test_noalloc_leaves_the_device_pool_untouched():
     marks = {}
     for name in ("noalloc", "ordinary"):
         base = _pool_attr(rt, pool, used)
-        assert rt.cudaMemPoolSetAttribute(pool, high, rt.cuuint64_t(0))[0] == rt.cudaError_t.cudaSuccess
+        assert rt.cudaMemPoolSetAttribute(pool, high, _u64(0))[0] == rt.cudaError_t.cudaSuccess
         fn = lib.rvvla_csr5_spmv_f64_noalloc if name == "noalloc" else lib.rvvla_csr5_spmv_f64
         assert fn(C.byref(d), 1.0, x.data_ptr(), 0.0, y.data_ptr(), st) == 0, lib.rvvla_last_error()
         torch.cuda.synchronize()
