@@ -175,9 +175,14 @@ lav_fused_kernel(int64_t nseg, int64_t cc, int64_t m, int64_t n, int64_t nlong, 
 constexpr int64_t kLavLongSteps = 128;
 
 
+}  // namespace
+
+// lav_build.cu
 template <class T>
 int lav_build_gpu(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen, int64_t long_steps,
                   rvvla_lav_owned* out, cudaStream_t st);
+
+namespace {
 
 template <class T>
 int lav_build_typed(const rvvla_crs* src, int64_t L, double Tthr, int64_t seglen, rvvla_lav_owned* out, cudaStream_t st) {
