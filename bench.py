@@ -347,7 +347,7 @@ def run_gpu(args):
     # across cases is reported beside it
     e2e_ms_py, h2d_py, d2h_py = e2e_time(cases, args, torch)
     e2e_ms_py = max_over_ranks(e2e_ms_py, world, "cuda")
-    drop = e2e_dropin(args, [c.name for c in cases], local)
+    drop = None if args.no_e2e else e2e_dropin(args, [c.name for c in cases], local)
     e2e_ms = max_over_ranks(drop["ms_per_step"] if drop else float("inf"), world, "cuda")
 
     pk = peaks()
@@ -393,7 +393,8 @@ def run_gpu(args):
                  "h2d_bytes_per_step": drop["h2d_bytes_per_step"], "d2h_bytes_per_step": drop["d2h_bytes_per_step"],
                  "ms_per_step": round(e2e_ms, 4), "path": "C++ drop-in sparse_mv / sparse_mv_mixed, host "
                  "std::vector b and y (pageable), one synchronous call per case", "per_case_ms": drop["per_case_ms"]}
-                if drop else {"value": None, "unit": "GB/s", "error": "drop-in harness unavailable"}),
+                if drop else {"value": None, "unit": "GB/s",
+                              "error": "skipped (--no-e2e)" if args.no_e2e else "drop-in harness unavailable"}),
         "e2e_python_pinned_overlapped": {"value": round(job_gbs(total_bytes, world, e2e_ms_py), 1), "unit": "GB/s",
                                          "h2d_bytes_per_step": h2d_py, "d2h_bytes_per_step": d2h_py,
                                          "ms_per_step": round(e2e_ms_py, 4)},
@@ -871,6 +872,8 @@ def main():
     ap.add_argument("--precisions", default="f64,f32,mixed")
     ap.add_argument("--cpu-iters", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the drop-in end-to-end leg (a child process; for profiling runs)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the precision (stencil), batched and adjoint forms reported under 'forms'")
     args = ap.parse_args()
