@@ -811,6 +811,63 @@ def cpu_parts(times: dict, ref_threads: int) -> dict:
     return out
 
 
+def run_sharded(args):
+    """--sharded: one product of the whole matrix split across the ranks
+    (rvvlasparse_b200.distributed.RowShardedCRS: nonzero-balanced row ranges,
+    the x halo exchanged over NCCL while the diagonal block multiplies) per
+    step, CRS fp64.  Strong scaling: the matrix is the same at every N;
+    value = the whole product's CRS bytes / the slowest rank's step time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import rvvlasparse_b200 as R
+    from rvvlasparse_b200.distributed import RowShardedCRS
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl" if world > 1 else "gloo", timeout=datetime.timedelta(seconds=120),
+                            **({} if world > 1 else {"init_method": "tcp://127.0.0.1:0", "rank": 0,
+                                                     "world_size": 1}))
+    try:
+        lib = R.load()
+        m, n, Rst, Col, Val = workload(args.workload, args.n)
+        S = RowShardedCRS(m, n, Rst, Col, Val, device="cuda", exchange=args.exchange)
+        x = torch.as_tensor(np.random.default_rng(0).uniform(-1, 1, n)[S.r0:S.r1].copy()).cuda()
+        y = torch.zeros(S.local_rows, dtype=torch.float64, device="cuda")
+        for _ in range(max(args.warmup, 3)):
+            S.spmv(x, 1.0, 0.0, y)
+        torch.cuda.synchronize()
+        dist.barrier()
+        l0 = lib.rvvla_kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            S.spmv(x, 1.0, 0.0, y)
+        e1.record()
+        torch.cuda.synchronize()
+        launches = lib.rvvla_kernel_launch_count() - l0
+        dist.barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda") if world > 1 else \
+            e0.elapsed_time(e1) / args.steps
+        byts = crs_bytes(m, n, len(Col), 8, 8)
+        exchanged = S.exchanged_per_spmv
+    finally:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": round(byts / (ms * 1e-3) / 1e9, 1), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload} n={m} nnz={len(Col)}", "cases": ["crs_f64_row_sharded"],
+                       "parallelism": f"rows{world}", "exchange": args.exchange,
+                       "x_entries_sent_by_rank0_per_step": exchanged},
+            "gpu_launches": int(launches)}), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -872,6 +929,11 @@ def main():
     ap.add_argument("--precisions", default="f64,f32,mixed")
     ap.add_argument("--cpu-iters", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="time one row-sharded CRS fp64 product across the ranks per step (strong scaling) "
+                         "instead of a replica of every case per rank")
+    ap.add_argument("--exchange", default="halo", choices=["halo", "allgather"],
+                    help="x exchange of --sharded")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the drop-in end-to-end leg (a child process; for profiling runs)")
     ap.add_argument("--no-forms", action="store_true",
@@ -883,6 +945,8 @@ def main():
         ap.error("--steps must be >= 1")
     if args.impl == "reference":
         run_reference(args)
+    elif args.sharded:
+        run_sharded(args)
     else:
         run_gpu(args)
 
