@@ -29,9 +29,16 @@
 //     are cut into rounds of 2048; every warp computes 128 products in stream
 //     order (the block of each nonzero from the compacted list: a warp-wide
 //     OR of the next block starts and a popcount), writes (row, product,
-//     owner) to shared memory, and after a barrier each owner warp picks its
-//     own nonzeros in stream order and adds them (nonzeros of one row inside a
-//     group of 32 are summed in lane order first).
+//     owner) to shared memory — a run of one row inside one block summed
+//     first, by a segmented warp scan — and after a barrier each owner warp
+//     picks its own run sums in stream order and adds them 32 at a time
+//     (COO rows belong to warps in interleaved chunks of 16 rows, so that
+//     the few hundred consecutive rows of a block spread over the warps;
+//     the CSR phase's row ranges are not needed here, since barriers
+//     separate the phases); lanes holding
+//     the same row add one after another in lane order (an integer atomicMin
+//     over a per-warp slot table elects the lowest pending lane of each row
+//     per round).
 // The next round's loads are issued before the current round is applied.
 // Per row, the sum is: CSR pieces of window 0 in block order, COO products of
 // window 0 in stream order, then window 1, ...; y = alpha*acc + beta*y at the
@@ -58,6 +65,7 @@ constexpr int kHW = kHT / 32;              // warps = row owners
 constexpr int kHWin = 2048;                // block columns per window
 constexpr int kHRound = 2048;              // COO nonzeros per round
 constexpr int kHU = kHRound / (kHW * 32);  // sub-steps of 32 per warp and round
+constexpr int kHSlots = 128;               // per-warp row slots of the COO apply (power of two)
 constexpr int kHLane = 8;                  // CSR nonzeros per lane and chunk
 constexpr int kHChunk = 32 * kHLane;
 
@@ -77,7 +85,7 @@ __host__ __device__ constexpr size_t hal16(size_t b) { return (b + 15) / 16 * 16
 // per-warp mark groups.
 template <class SA, class P>
 struct HLayout {
-  size_t acc, list, prod, row, own, wscr, mgrp, total;
+  size_t acc, list, prod, row, own, wscr, mgrp, slot, total;
   __host__ __device__ explicit HLayout(int64_t racc) {
     acc = 0;
     list = hal16((size_t)racc * sizeof(SA));
@@ -86,16 +94,24 @@ struct HLayout {
     own = row + (size_t)kHRound * 4;
     wscr = own + hal16((size_t)kHRound);
     mgrp = wscr + (size_t)kHW * 1024;
-    total = mgrp + (size_t)kHW * 32 * 4;
+    slot = mgrp + (size_t)kHW * 32 * 4;
+    total = slot + (size_t)kHW * kHSlots * 4;
   }
 };
 
 template <class V, class X, class SA, bool MIX>
 struct HTypes {
-  using Ac = std::conditional_t<MIX, CompF32, SA>;                        // CSR lane sums
-  using P = std::conditional_t<(MIX || sizeof(SA) == 4), float, double>;  // a COO product
-  using PT = decltype(vmul(V(), X()));                                    // a CSR product
+  using Ac = std::conditional_t<MIX, CompF32, SA>;  // CSR lane sums
+  using P = SA;                                     // a COO run sum (fp64 in the mixed forms)
+  using PT = decltype(vmul(V(), X()));              // a product
 };
+
+// COO rows belong to warps in chunks of 16 consecutive rows, interleaved
+// (a block of a few hundred consecutive rows spreads over the warps)
+__device__ __forceinline__ uint32_t hcsr_coo_owner(uint32_t r) { return (r >> 4) & (kHW - 1); }
+// the slot of an owned row in its warp's table: distinct for 2048
+// consecutive rows
+__device__ __forceinline__ uint32_t hcsr_coo_slot(uint32_t r) { return (((r >> 8) << 4) | (r & 15)) & (kHSlots - 1); }
 
 // Exclusive CTA-wide scan of three counters; t* are the CTA totals.
 __device__ __forceinline__ void hcsr_scan3(int a, int b, int c, int& pa, int& pb, int& pc, int& ta, int& tb,
@@ -300,9 +316,11 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
   int* table = reinterpret_cast<int*>(smem + L.wscr + (size_t)warp * 1024);          // CSR phase
   uint16_t* olist = reinterpret_cast<uint16_t*>(smem + L.wscr + (size_t)warp * 1024);  // COO phase
   uint32_t* mgrp = reinterpret_cast<uint32_t*>(smem + L.mgrp) + warp * 32;
+  int* slot = reinterpret_cast<int*>(smem + L.slot) + warp * kHSlots;
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
 
   for (int li = tid; li < rows; li += kHT) acc[li] = SA(0);
+  for (int q = lane; q < kHSlots; q += 32) slot[q] = INT_MAX;
   // this warp's rows
   const int ra = (int)(((int64_t)warp * rows + kHW - 1) / kHW);
   const int rb = (int)(((int64_t)(warp + 1) * rows + kHW - 1) / kHW);
@@ -399,6 +417,8 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
           const int q = q0 + lane;
           HCooRaw<V>& r = raw[u];
           r.ok = q < ntot;
+          r.row = 0u;
+          r.xoff = -1;
           if (r.ok) {
             const HBlk h = list[blk];
             const int e = q - h.cs;
@@ -414,21 +434,31 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
       coo_load(0);
       for (int t = 0; t < nrounds; ++t) {
         // products of this round into shared memory, in stream order
+        X xv[kHU];
+#pragma unroll
+        for (int u = 0; u < kHU; ++u) xv[u] = raw[u].ok ? ld_keep(x + raw[u].xoff + raw[u].col, pl) : X(0);
 #pragma unroll
         for (int u = 0; u < kHU; ++u) {
           const int i = warp * (kHU * 32) + 32 * u + lane;
           const HCooRaw<V>& r = raw[u];
           P pv = P(0);
-          uint32_t own = 0xFFu;
           if (r.ok) {
-            const X xv = ld_keep(x + r.xoff + r.col, pl);
-            if constexpr (MIX) pv = to_f32(r.v) * (float)xv;
-            else pv = (P)(r.v * xv);
-            own = (uint32_t)(((int64_t)kHW * r.row) / rows);
+            if constexpr (MIX) pv = (P)(to_f32(r.v) * (float)xv[u]);
+            else pv = (P)(r.v * xv[u]);
           }
-          s_prod[i] = pv;
-          s_row[i] = r.ok ? r.row : 0u;
-          s_own[i] = (uint8_t)own;
+          // runs of one row inside one block (consecutive lanes) are summed
+          // here; only the run's last lane is handed on
+          const uint32_t prow = __shfl_up_sync(0xffffffffu, r.row, 1);
+          const int64_t pxo = __shfl_up_sync(0xffffffffu, r.xoff, 1);
+          const bool head = lane == 0 || !r.ok || prow != r.row || pxo != r.xoff;
+          const P run = warp_seg_scan(pv, head, lane);
+          const uint32_t nrow = __shfl_down_sync(0xffffffffu, r.row, 1);
+          const int64_t nxo = __shfl_down_sync(0xffffffffu, r.xoff, 1);
+          const bool nok = __shfl_down_sync(0xffffffffu, r.ok, 1);
+          const bool tail = r.ok && (lane == 31 || !nok || nrow != r.row || nxo != r.xoff);
+          s_prod[i] = run;
+          s_row[i] = r.row;
+          s_own[i] = (uint8_t)(tail ? hcsr_coo_owner(r.row) : 0xFFu);
         }
         __syncthreads();
         if (t + 1 < nrounds) coo_load(t + 1);
@@ -459,26 +489,33 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
             m16 &= m16 - 1u;
           }
           __syncwarp();
+          // groups of 32 of this warp's nonzeros; inside a group, rounds in
+          // which the lowest pending lane of every row slot adds its value
+          // (an integer atomicMin elects it), so each row receives its
+          // values in lane order = stream order, whatever the scheduling
           for (int g = 0; g < total; g += 32) {
             const int tt = g + lane;
-            uint32_t r = 0xFFFFFFFFu;
+            bool pend = tt < total;
+            uint32_t r = 0;
             SA pv = SA(0);
-            if (tt < total) {
+            if (pend) {
               const int i = olist[tt];
               r = s_row[i];
               pv = (SA)s_prod[i];
             }
-            const unsigned peers = __match_any_sync(0xffffffffu, r);
-            const int np = __popc(peers);
-            const int maxnp = (int)__reduce_max_sync(0xffffffffu, (unsigned)np);
-            SA s = pv;
-            for (int k = 1; k < maxnp; ++k) {  // the row's other values, in lane order
-              const int src = k < np ? (int)__fns(peers, 0, k + 1) : lane;
-              const SA ov = __shfl_sync(0xffffffffu, pv, src);
-              if (k < np) s += ov;
+            int* sl = slot + hcsr_coo_slot(r);
+            while (__ballot_sync(0xffffffffu, pend)) {
+              if (pend) atomicMin(sl, lane);
+              __syncwarp();
+              const bool win = pend && *sl == lane;
+              __syncwarp();
+              if (win) {
+                acc[r] += pv;
+                *sl = INT_MAX;
+                pend = false;
+              }
+              __syncwarp();
             }
-            if (tt < total && lane == __ffs(peers) - 1) acc[r] += s;
-            __syncwarp();
           }
         }
         __syncthreads();
