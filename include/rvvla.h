@@ -275,7 +275,8 @@ typedef struct rvvla_lav_owned {
   int32_t* sp_plan; /* rvvla_crs_analyze plan of sparse_part (the builder sets h.sparse_part.plan) */
 } rvvla_lav_owned;
 
-/* Builder (the reference has none; built on the host, then uploaded): dense
+/* Builder (the reference has none; built on the GPU with stable radix sorts,
+ * only the few scalars of the plan pass through the host): dense
  * columns = the most populated columns holding >= (1-T) of the nonzeros,
  * segments of segment_len of them; rows chunked by dense count, descending;
  * inside a chunk each segment orders rows by their count in that segment.
@@ -347,7 +348,9 @@ typedef struct rvvla_vnec_owned {
 
 /* spMtxVNEC(const spMtxCRS&) (include/VNEC.h:200-227): partition, x
  * compaction, IRD and variant choice, plus the S/D structures the
- * reference's kernels read (built on the host, then uploaded).  nthreads <= 0
+ * reference's kernels read (built on the GPU: merge-path partition, compaction
+ * by a stable radix sort, per-group and per-task scans; the IRD and the
+ * variant choice read a few scalars back).  nthreads <= 0
  * picks one merge tile (2048 items) per thread; variant -1 applies the
  * reference's rule, 0/1/2 force D/S/L.  val_bytes 8 or 4.  Synchronises
  * `stream`. */

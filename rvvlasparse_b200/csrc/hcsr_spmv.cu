@@ -15,33 +15,38 @@
 // the result is bitwise reproducible run to run (no float atomics).
 //
 // The block columns are taken in windows of kHWin blocks: the window's
-// non-empty blocks are compacted into a CSR list and a COO list in shared
-// memory (so the metadata staged never depends on b_n), then
-//   * CSR phase: each warp walks every CSR block of the window for its own
-//     rows: their nonzeros are one contiguous range, streamed in chunks of
-//     256 (8 consecutive nonzeros per lane, 16-byte loads of values and
-//     uint16 columns); the rows starting inside a chunk are marked from the
-//     block's row_ptr (a window of 32 row starts per lane set, prefetched one
+// non-empty blocks are compacted into a row-range list and a COO list in
+// shared memory (so the metadata staged never depends on b_n), then
+//   * row-range phase: each warp walks, in block order, every CSR block and
+//     every COO block of at least kHBig nonzeros for its own rows.  A CSR
+//     block's nonzeros of those rows are one contiguous range, streamed in
+//     chunks of 256 (8 consecutive nonzeros per lane, 16-byte loads of values
+//     and uint16 columns); the rows starting inside a chunk are marked from
+//     the block's row_ptr (a window of 32 row starts per lane set, loaded one
 //     window ahead), each lane sums its 8 products split at the marks, and a
 //     reverse segmented warp scan closes the rows that cross lanes, so each
-//     row piece of a chunk is added to the accumulator exactly once;
-//   * COO phase: the window's COO nonzeros (all COO blocks, in block order)
-//     are cut into rounds of 2048; every warp computes 128 products in stream
-//     order (the block of each nonzero from the compacted list: a warp-wide
-//     OR of the next block starts and a popcount), writes (row, product,
-//     owner) to shared memory — a run of one row inside one block summed
-//     first, by a segmented warp scan — and after a barrier each owner warp
-//     picks its own run sums in stream order and adds them 32 at a time
-//     (COO rows belong to warps in interleaved chunks of 16 rows, so that
-//     the few hundred consecutive rows of a block spread over the warps;
-//     the CSR phase's row ranges are not needed here, since barriers
-//     separate the phases); lanes holding
-//     the same row add one after another in lane order (an integer atomicMin
-//     over a per-warp slot table elects the lowest pending lane of each row
-//     per round).
+//     row piece of a chunk is added to the accumulator exactly once.  A large
+//     COO block keeps its nonzeros in row order (the builder writes them so):
+//     the warp finds its range by a 32-ary search on the rows and streams it
+//     the same way, a row starting wherever the row changes; a CTA that finds
+//     rows out of order there starts its block row over with every COO block
+//     in the COO phase;
+//   * COO phase: the window's other COO nonzeros (in block order) are cut
+//     into rounds of 2048; every warp computes 128 products in stream order
+//     (the block of each nonzero from the compacted list: a warp-wide OR of
+//     the next block starts and a popcount), writes (row, product, owner) to
+//     shared memory — a run of one row inside one block summed first, by a
+//     segmented warp scan — and after a barrier each owner warp picks its own
+//     run sums in stream order and adds them 32 at a time (COO rows belong to
+//     warps in interleaved chunks of 16 rows, so that the few hundred
+//     consecutive rows of a block spread over the warps; the row-range
+//     phase's ranges are not needed here, since barriers separate the
+//     phases); lanes holding the same row add one after another in lane
+//     order (an integer atomicMin over a per-warp slot table elects the
+//     lowest pending lane of each row per round).
 // The next round's loads are issued before the current round is applied.
-// Per row, the sum is: CSR pieces of window 0 in block order, COO products of
-// window 0 in stream order, then window 1, ...; y = alpha*acc + beta*y at the
+// Per row, the sum is: row-range pieces of window 0 in block order, COO
+// products of window 0 in stream order, then window 1, ...; y = alpha*acc + beta*y at the
 // end (y is not read when beta == 0).
 //
 // Mixed forms: lane sums of the CSR phase in compensated fp32 (two-sum), COO
@@ -60,14 +65,19 @@ namespace rvvla {
 namespace {
 
 constexpr uint32_t kHKindMask = 0x3FFFFFFFu;
-constexpr int kHT = 512;                   // threads per CTA
-constexpr int kHW = kHT / 32;              // warps = row owners
-constexpr int kHWin = 2048;                // block columns per window
+constexpr int kHW = 16;                    // warps per CTA = row owners
+constexpr int kHT = 32 * kHW;              // threads per CTA
+constexpr int kHMinBlocks = 2;             // resident CTAs per SM the registers are sized for
+constexpr int kHWLog = kHW == 8 ? 3 : 4;
+static_assert(kHW == 8 || kHW == 16, "8 or 16 row owners");
+constexpr int kHWin = 4 * kHT;             // block columns per window (4 per thread)
 constexpr int kHRound = 2048;              // COO nonzeros per round
 constexpr int kHU = kHRound / (kHW * 32);  // sub-steps of 32 per warp and round
-constexpr int kHSlots = 128;               // per-warp row slots of the COO apply (power of two)
+constexpr int kHSlots = 2048 / kHW;        // per-warp row slots of the COO apply (power of two)
+constexpr int kHBig = 1024;                // COO blocks of at least this many nonzeros take the row-range path
 constexpr int kHLane = 8;                  // CSR nonzeros per lane and chunk
 constexpr int kHChunk = 32 * kHLane;
+constexpr int kHWscr = kHChunk * 4 > 1024 ? kHChunk * 4 : 1024;  // per-warp scratch bytes
 
 // a non-empty block of the window: COO stream start (COO list only), nonzero
 // offset, row_ptr offset, block column
@@ -93,7 +103,7 @@ struct HLayout {
     row = prod + hal16((size_t)kHRound * sizeof(P));
     own = row + (size_t)kHRound * 4;
     wscr = own + hal16((size_t)kHRound);
-    mgrp = wscr + (size_t)kHW * 1024;
+    mgrp = wscr + (size_t)kHW * kHWscr;
     slot = mgrp + (size_t)kHW * 32 * 4;
     total = slot + (size_t)kHW * kHSlots * 4;
   }
@@ -109,9 +119,11 @@ struct HTypes {
 // COO rows belong to warps in chunks of 16 consecutive rows, interleaved
 // (a block of a few hundred consecutive rows spreads over the warps)
 __device__ __forceinline__ uint32_t hcsr_coo_owner(uint32_t r) { return (r >> 4) & (kHW - 1); }
-// the slot of an owned row in its warp's table: distinct for 2048
+// the slot of an owned row in its warp's table: distinct for 16 * kHSlots
 // consecutive rows
-__device__ __forceinline__ uint32_t hcsr_coo_slot(uint32_t r) { return (((r >> 8) << 4) | (r & 15)) & (kHSlots - 1); }
+__device__ __forceinline__ uint32_t hcsr_coo_slot(uint32_t r) {
+  return (((r >> (4 + kHWLog)) << 4) | (r & 15)) & (kHSlots - 1);
+}
 
 // Exclusive CTA-wide scan of three counters; t* are the CTA totals.
 __device__ __forceinline__ void hcsr_scan3(int a, int b, int c, int& pa, int& pb, int& pc, int& ta, int& tb,
@@ -156,13 +168,32 @@ __device__ __forceinline__ void hcsr_scan3(int a, int b, int c, int& pa, int& pb
 }
 
 // eight uint16 columns with one 16-byte load
-__device__ __forceinline__ void hcsr_cols8(const uint16_t* p, uint32_t (&c)[kHLane], uint64_t pol) {
-  const int4 t = ld_v4_l1(p, pol);
-  const uint32_t w[4] = {(uint32_t)t.x, (uint32_t)t.y, (uint32_t)t.z, (uint32_t)t.w};
+// kHLane uint16 columns with 16-byte loads
+__device__ __forceinline__ void hcsr_cols(const uint16_t* p, uint32_t (&c)[kHLane], uint64_t pol) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    c[2 * q] = w[q] & 0xFFFFu;
-    c[2 * q + 1] = w[q] >> 16;
+  for (int h = 0; h < kHLane / 8; ++h) {
+    const int4 t = ld_v4_l1(p + 8 * h, pol);
+    const uint32_t w[4] = {(uint32_t)t.x, (uint32_t)t.y, (uint32_t)t.z, (uint32_t)t.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      c[8 * h + 2 * q] = w[q] & 0xFFFFu;
+      c[8 * h + 2 * q + 1] = w[q] >> 16;
+    }
+  }
+}
+
+// kHLane values with 16-byte loads
+template <class V>
+__device__ __forceinline__ void hcsr_vals(const V* p, V (&v)[kHLane], uint64_t pol) {
+  constexpr int E = 16 / (int)sizeof(V);  // values per load
+#pragma unroll
+  for (int q = 0; q < kHLane / E; ++q) {
+    const int4 t = ld_v4_l1(p + E * q, pol);
+    V tmp[E];
+    static_assert(sizeof(tmp) == sizeof(int4), "one 16-byte load");
+    memcpy(tmp, &t, sizeof(int4));
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[E * q + e] = tmp[e];
   }
 }
 
@@ -177,11 +208,164 @@ __device__ __forceinline__ void hcsr_add(SA* acc, int r, T v) {
   acc[r] += (SA)v;
 }
 
-// CSR phase of one warp for one CSR block: rows [ra, rb) of the block, whose
-// nonzeros are [lo, hi) (absolute).  Row starts come from rp (the block's
-// row_ptr, block-relative) in windows of 32 rows.
+// Row-range phase of one warp for one CSR block: the nonzeros of the warp's
+// rows [ra, rb).  Chunks of kHChunk nonzeros, kHLane consecutive ones per
+// lane (16-byte loads): positions count from the block's first nonzero
+// rounded down to a multiple of 8, so a chunk start is 16-byte aligned
+// whenever the arrays are (VEC).  Row starts come from the block's row_ptr
+// in windows of 32 rows (the next window loaded one window ahead) and mark
+// the lanes' slots through a per-warp table; each lane sums its products
+// split at the marks, and a reverse segmented scan adds the parts of rows
+// crossing lanes.  When no lane holds two row starts (rows of 8 or more
+// nonzeros), a lane's sums take the branch-free split at its one mark.
 template <class V, class X, class SA, bool MIX, bool VEC>
-__device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t lo,
+__device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t nz,
+                                              const uint16_t* __restrict__ col_idx, const V* __restrict__ values,
+                                              const X* __restrict__ xb, SA* acc, int* table, uint32_t* mgrp, int lane,
+                                              uint64_t pf, uint64_t pl) {
+  using Ty = HTypes<V, X, SA, MIX>;
+  using Ac = typename Ty::Ac;
+  using PT = typename Ty::PT;
+  using CT = SA;
+  const int64_t base = bp & ~(int64_t)7;
+  const uint32_t off = (uint32_t)(bp - base);
+  const uint32_t lo = off + __ldg(rp + ra), hi = off + __ldg(rp + rb);
+  if (lo >= hi) return;
+  const uint32_t lim = (uint32_t)(nz - base);  // positions below lim lie inside the arrays
+  const V* __restrict__ vb = values + base;
+  const uint16_t* __restrict__ cb = col_idx + base;
+  int wb = ra;
+  auto ldwin = [&](int b0, uint32_t& s, uint32_t& e) {
+    const int r = b0 + lane;
+    s = r < rb ? off + __ldg(rp + r) : 0xFFFFFFFFu;
+    e = r < rb ? off + __ldg(rp + r + 1) : 0xFFFFFFFFu;
+  };
+  uint32_t s_c, e_c, s_n, e_n;
+  ldwin(wb, s_c, e_c);
+  ldwin(wb + 32, s_n, e_n);
+  int open_row = -1;
+  for (uint32_t c = lo & ~7u; c < hi; c += kHChunk) {
+    const uint32_t a = c + kHLane * lane;
+    const uint32_t fv = lo > a ? lo - a : 0u;  // the lane's slots in [fv, lv) lie in [lo, hi)
+    const uint32_t lv = hi > a ? hi - a : 0u;
+    // ---- loads and products
+    PT p[kHLane];
+    {
+      V vv[kHLane];
+      uint32_t cc[kHLane];
+      if (VEC && a + kHLane <= lim) {
+        hcsr_vals(vb + a, vv, pf);
+        hcsr_cols(cb + a, cc, pf);
+      } else {
+#pragma unroll
+        for (int i = 0; i < kHLane; ++i) {
+          const bool in = a + i < lim;
+          vv[i] = in ? hcsr_ld1(vb + a + i) : V(0);
+          cc[i] = in ? (uint32_t)__ldg(cb + a + i) : 0u;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) {
+        const bool ok = (uint32_t)i >= fv && (uint32_t)i < lv;
+        if constexpr (MIX) p[i] = ok ? to_f32(vv[i]) * (float)ld_keep(xb + cc[i], pl) : 0.f;
+        else p[i] = ok ? vv[i] * ld_keep(xb + cc[i], pl) : PT(0);
+      }
+    }
+    // ---- marks of the rows that start inside the chunk
+    mgrp[lane] = 0u;
+    __syncwarp();
+    for (;;) {
+      const uint32_t pos = s_c - c;  // wraps for rows that started before the chunk
+      if (pos < (uint32_t)kHChunk && s_c < e_c) {
+        table[pos] = wb + lane;
+        atomicOr(mgrp + pos / kHLane, 1u << (pos % kHLane));
+      }
+      const uint32_t s31 = __shfl_sync(0xffffffffu, s_c, 31);
+      if (!(wb + 32 < rb && s31 < c + kHChunk)) break;
+      wb += 32;
+      s_c = s_n;
+      e_c = e_n;
+      ldwin(wb + 32, s_n, e_n);
+    }
+    __syncwarp();
+    const uint32_t mb = mgrp[lane];
+    // ---- lane sums: lead = before the lane's first mark, sum = from its last
+    // mark; rows that start and end inside the lane are added now
+    Ac sum, lead;
+    acc_zero(sum);
+    acc_zero(lead);
+    int nf = 0, rcur = -1;
+    if (!__any_sync(0xffffffffu, (mb & (mb - 1u)) != 0u)) {
+      const int m = mb ? __ffs(mb) - 1 : kHLane;
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) {
+        if (i < m) acc_add(lead, p[i]);
+        else acc_add(sum, p[i]);
+      }
+      if (mb) {
+        nf = 1;
+        rcur = table[kHLane * lane + m];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) {
+        if ((mb >> i) & 1u) {
+          if (nf == 0) lead = sum;
+          else hcsr_add(acc, rcur, acc_carry(sum));
+          rcur = table[kHLane * lane + i];
+          ++nf;
+          acc_zero(sum);
+        }
+        acc_add(sum, p[i]);
+      }
+      if (nf == 0) lead = sum;
+    }
+    // ---- rows crossing lanes: reverse segmented scan of the leads
+    const unsigned marks = __ballot_sync(0xffffffffu, nf > 0);
+    const unsigned ge = marks & (~0u << lane);
+    const int e = ge ? __ffs(ge) - 1 : 31;
+    CT T = (CT)acc_carry(lead);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const CT o = __shfl_down_sync(0xffffffffu, T, d);
+      if (lane + d <= e) T += o;
+    }
+    CT Tn = __shfl_down_sync(0xffffffffu, T, 1);
+    if (lane == 31) Tn = CT(0);
+    const CT T0 = __shfl_sync(0xffffffffu, T, 0);
+    if (lane == 0 && open_row >= 0) hcsr_add(acc, open_row, T0);
+    if (nf > 0) hcsr_add(acc, rcur, (CT)acc_carry(sum) + Tn);
+    if (marks) open_row = __shfl_sync(0xffffffffu, rcur, 31 - __clz(marks));
+    __syncwarp();
+  }
+}
+
+// First k in [0, cnt) with rows[k] >= t (cnt when none), for ascending rows;
+// a 32-ary search of the warp (each step probes 32 positions).  On rows that
+// do not ascend the result is some k in [0, cnt].
+__device__ __forceinline__ int hcsr_lower_bound(const uint32_t* __restrict__ rows, int cnt, uint32_t t, int lane) {
+  int lo = 0, hi = cnt;  // the answer lies in [lo, hi]
+  while (hi - lo > 32) {
+    const int k = lo + (int)(((int64_t)(hi - lo) * lane) >> 5);
+    const int c = __popc(__ballot_sync(0xffffffffu, __ldg(rows + k) < t));
+    const int nlo = c > 0 ? __shfl_sync(0xffffffffu, k, (c - 1) & 31) + 1 : lo;
+    const int nhi = c < 32 ? __shfl_sync(0xffffffffu, k, c & 31) : hi;
+    lo = nlo;
+    hi = max(nhi, nlo);
+  }
+  const bool less = lo + lane < hi && __ldg(rows + lo + lane) < t;
+  return lo + __popc(__ballot_sync(0xffffffffu, less));
+}
+
+// Row-range phase of one warp for one block: the nonzeros [lo, hi)
+// (absolute) of the warp's rows [ra, rb).  CSR block (COO = false): row starts
+// come from rp (the block's row_ptr, block-relative) in windows of 32 rows.
+// COO block (COO = true): rp holds each nonzero's row (rp[k - bp]); a row
+// starts where the row differs from the previous nonzero's.  Returns true
+// (COO only) when a row descends or lies outside [ra, rb); such nonzeros are
+// left out.
+template <class V, class X, class SA, bool MIX, bool VEC, bool COO>
+__device__ __forceinline__ bool hcsr_seg_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t lo,
                                               int64_t hi, int64_t nz, const uint16_t* __restrict__ col_idx,
                                               const V* __restrict__ values, const X* __restrict__ xb, SA* acc,
                                               int* table, uint32_t* mgrp, int lane, uint64_t pf, uint64_t pl) {
@@ -197,12 +381,35 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
     s = r < rb ? __ldg(rp + r) : 0xFFFFFFFFu;
     e = r < rb ? __ldg(rp + r + 1) : 0xFFFFFFFFu;
   };
-  uint32_t s_c, e_c, s_n, e_n;
-  ldwin(wb, s_c, e_c);
-  ldwin(wb + 32, s_n, e_n);
+  uint32_t s_c = 0, e_c = 0, s_n = 0, e_n = 0;
+  if constexpr (!COO) {
+    ldwin(wb, s_c, e_c);
+    ldwin(wb + 32, s_n, e_n);
+  }
+  uint32_t last_row = 0xFFFFFFFFu;   // COO: row of the last nonzero before the chunk
+  uint32_t last_kept = 0xFFFFFFFFu;  // COO: the same, of the kept nonzeros
+  bool bad = false;
   int open_row = -1;
   for (int64_t c = lo & ~(int64_t)7; c < hi; c += kHChunk) {
     const int64_t a = c + kHLane * lane;
+    // ---- COO: rows (0xFFFFFFFF outside [lo, hi) and outside [ra, rb))
+    uint32_t rw[kHLane];
+    if constexpr (COO) {
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) rw[i] = a + i >= lo && a + i < hi ? __ldg(rp + (a + i - bp)) : 0xFFFFFFFFu;
+      uint32_t before = __shfl_up_sync(0xffffffffu, rw[kHLane - 1], 1);
+      if (lane == 0) before = last_row;
+      const uint32_t l31 = __shfl_sync(0xffffffffu, rw[kHLane - 1], 31);
+      last_row = l31 != 0xFFFFFFFFu ? l31 : last_row;
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) {
+        if (rw[i] != 0xFFFFFFFFu) {
+          if ((before != 0xFFFFFFFFu && rw[i] < before) || rw[i] < (uint32_t)ra || rw[i] >= (uint32_t)rb) bad = true;
+          before = rw[i];
+          if (rw[i] < (uint32_t)ra || rw[i] >= (uint32_t)rb) rw[i] = 0xFFFFFFFFu;
+        }
+      }
+    }
     // ---- loads and products
     PT p[kHLane];
     {
@@ -210,8 +417,8 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
       uint32_t cc[kHLane];
       const bool any = a < hi && a + kHLane > lo;
       if (VEC && any && a + kHLane <= nz) {
-        RunVec<V>::load(values + a, vv, pf);
-        hcsr_cols8(col_idx + a, cc, pf);
+        hcsr_vals(values + a, vv, pf);
+        hcsr_cols(col_idx + a, cc, pf);
       } else {
 #pragma unroll
         for (int i = 0; i < kHLane; ++i) {
@@ -222,30 +429,44 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
       }
 #pragma unroll
       for (int i = 0; i < kHLane; ++i) {
-        const bool ok = a + i >= lo && a + i < hi;
+        const bool ok = COO ? rw[i] != 0xFFFFFFFFu : a + i >= lo && a + i < hi;
         if constexpr (MIX) p[i] = ok ? to_f32(vv[i]) * (float)ld_keep(xb + cc[i], pl) : 0.f;
         else p[i] = ok ? vv[i] * ld_keep(xb + cc[i], pl) : PT(0);
       }
     }
     // ---- marks of the rows that start inside the chunk
-    mgrp[lane] = 0u;
-    __syncwarp();
-    for (;;) {
-      const int64_t pos = bp + (int64_t)s_c - c;
-      if (wb + lane < rb && pos >= 0 && pos < kHChunk && s_c < e_c) {
-        table[pos] = wb + lane;
-        atomicOr(mgrp + (pos >> 3), 1u << (pos & 7));
+    uint32_t mb = 0;
+    if constexpr (COO) {
+      // a row starts where it differs from the previous kept nonzero's
+      uint32_t prev = __shfl_up_sync(0xffffffffu, rw[kHLane - 1], 1);
+      if (lane == 0) prev = last_kept;
+#pragma unroll
+      for (int i = 0; i < kHLane; ++i) {
+        const uint32_t before = i == 0 ? prev : rw[i - 1];
+        if (rw[i] != 0xFFFFFFFFu && rw[i] != before) mb |= 1u << i;
       }
-      const uint32_t s31 = __shfl_sync(0xffffffffu, s_c, 31);
-      const bool exhausted = wb + 32 < rb && bp + (int64_t)s31 - c < kHChunk;
-      if (!exhausted) break;
-      wb += 32;
-      s_c = s_n;
-      e_c = e_n;
-      ldwin(wb + 32, s_n, e_n);
+      const uint32_t k31 = __shfl_sync(0xffffffffu, rw[kHLane - 1], 31);
+      last_kept = k31 != 0xFFFFFFFFu ? k31 : last_kept;
+    } else {
+      mgrp[lane] = 0u;
+      __syncwarp();
+      for (;;) {
+        const int64_t pos = bp + (int64_t)s_c - c;
+        if (wb + lane < rb && pos >= 0 && pos < kHChunk && s_c < e_c) {
+          table[pos] = wb + lane;
+          atomicOr(mgrp + pos / kHLane, 1u << (pos % kHLane));
+        }
+        const uint32_t s31 = __shfl_sync(0xffffffffu, s_c, 31);
+        const bool exhausted = wb + 32 < rb && bp + (int64_t)s31 - c < kHChunk;
+        if (!exhausted) break;
+        wb += 32;
+        s_c = s_n;
+        e_c = e_n;
+        ldwin(wb + 32, s_n, e_n);
+      }
+      __syncwarp();
+      mb = mgrp[lane];
     }
-    __syncwarp();
-    const uint32_t mb = mgrp[lane];
     // ---- lane sums split at the marks; rows closed inside the lane are added now
     Ac sum, lead;
     acc_zero(sum);
@@ -256,7 +477,8 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
       if ((mb >> i) & 1u) {
         if (nf == 0) lead = sum;
         else hcsr_add(acc, rcur, acc_carry(sum));
-        rcur = table[kHLane * lane + i];
+        if constexpr (COO) rcur = (int)rw[i];
+        else rcur = table[kHLane * lane + i];
         ++nf;
         acc_zero(sum);
       }
@@ -281,6 +503,7 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
     if (marks) open_row = __shfl_sync(0xffffffffu, rcur, 31 - __clz(marks));
     __syncwarp();
   }
+  return bad;
 }
 
 // Raw loads of one COO sub-step (32 consecutive COO nonzeros of the window).
@@ -294,7 +517,7 @@ struct HCooRaw {
 };
 
 template <class V, class X, class SA, bool MIX, bool VEC, bool GACC>
-__global__ void __launch_bounds__(kHT, 2)
+__global__ void __launch_bounds__(kHT, kHMinBlocks)
 hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const int* __restrict__ block_ptr,
                  const uint32_t* __restrict__ row_offset, const uint32_t* __restrict__ row_ptr,
                  const uint16_t* __restrict__ col_idx, const V* __restrict__ values, const X* __restrict__ x,
@@ -313,77 +536,104 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
   P* s_prod = reinterpret_cast<P*>(smem + L.prod);
   uint32_t* s_row = reinterpret_cast<uint32_t*>(smem + L.row);
   uint8_t* s_own = smem + L.own;
-  int* table = reinterpret_cast<int*>(smem + L.wscr + (size_t)warp * 1024);          // CSR phase
-  uint16_t* olist = reinterpret_cast<uint16_t*>(smem + L.wscr + (size_t)warp * 1024);  // COO phase
+  int* table = reinterpret_cast<int*>(smem + L.wscr + (size_t)warp * kHWscr);          // CSR phase
+  uint16_t* olist = reinterpret_cast<uint16_t*>(smem + L.wscr + (size_t)warp * kHWscr);  // COO phase
   uint32_t* mgrp = reinterpret_cast<uint32_t*>(smem + L.mgrp) + warp * 32;
+  __shared__ int s_bad;  // a large COO block whose rows do not ascend was met
+  bool big_ok = true;
   int* slot = reinterpret_cast<int*>(smem + L.slot) + warp * kHSlots;
   const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
 
   for (int li = tid; li < rows; li += kHT) acc[li] = SA(0);
   for (int q = lane; q < kHSlots; q += 32) slot[q] = INT_MAX;
+  if (tid == 0) s_bad = 0;
   // this warp's rows
   const int ra = (int)(((int64_t)warp * rows + kHW - 1) / kHW);
   const int rb = (int)(((int64_t)(warp + 1) * rows + kHW - 1) / kHW);
   const int64_t blk0 = br * b_n;
   __syncthreads();
 
+  for (;;) {
   for (int64_t jw = 0; jw < b_n; jw += kHWin) {
     const int nb = (int)(b_n - jw < kHWin ? b_n - jw : kHWin);
-    // ---- compact the window's non-empty blocks (4 consecutive per thread)
+    // ---- compact the window's non-empty blocks (4 consecutive per thread):
+    // CSR blocks and COO blocks of >= kHBig nonzeros form the row-range list
+    // (block order, from the back of `list`), the smaller COO blocks the COO
+    // stream (from the front, with a sentinel)
     int bpq[4], cntq[4];
     uint32_t roq[4];
-    int n_csr = 0, n_coo = 0, n_ent = 0;
+    int kindq[4];  // 0 none, 1 CSR, 2 large COO, 3 small COO
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int jj = 4 * tid + q;
       bpq[q] = 0;
       cntq[q] = 0;
       roq[q] = 0u;
+      kindq[q] = 0;
       if (jj < nb) {
         const int64_t b = blk0 + jw + jj;
         bpq[q] = block_ptr[b];
         cntq[q] = block_ptr[b + 1] - bpq[q];
         roq[q] = row_offset[b];
-        if (cntq[q] > 0) {
-          if ((roq[q] >> 30) == 1u) ++n_csr;
-          else {
-            ++n_coo;
-            n_ent += cntq[q];
-          }
-        }
+        if (cntq[q] > 0) kindq[q] = (roq[q] >> 30) == 1u ? 1 : (cntq[q] >= kHBig && big_ok ? 2 : 3);
       }
     }
-    int p_csr, p_coo, p_ent, t_csr, t_coo, t_ent;
-    hcsr_scan3(n_csr, n_coo, n_ent, p_csr, p_coo, p_ent, t_csr, t_coo, t_ent, s_w);
+    int n_seg = 0, n_coo = 0, n_ent = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      if (cntq[q] > 0) {
-        HBlk h;
-        h.bp = bpq[q];
-        h.off = roq[q] & kHKindMask;
-        h.j = (int)(jw + 4 * tid + q);
-        if ((roq[q] >> 30) == 1u) {
-          h.cs = 0;
-          list[kHWin + 1 - t_csr + p_csr++] = h;
-        } else {
-          h.cs = p_ent;
-          p_ent += cntq[q];
-          list[p_coo++] = h;
-        }
+      if (kindq[q] == 1 || kindq[q] == 2) ++n_seg;
+      if (kindq[q] == 3) {
+        ++n_coo;
+        n_ent += cntq[q];
+      }
+    }
+    int p_seg, p_coo, p_ent, t_seg, t_coo, t_ent;
+    hcsr_scan3(n_seg, n_coo, n_ent, p_seg, p_coo, p_ent, t_seg, t_coo, t_ent, s_w);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (kindq[q] == 0) continue;
+      HBlk h;
+      h.bp = bpq[q];
+      h.off = roq[q] & kHKindMask;
+      h.j = (int)(jw + 4 * tid + q);
+      if (kindq[q] == 1 || kindq[q] == 2) {
+        h.cs = kindq[q] == 1 ? -1 : cntq[q];  // a large COO block keeps its nonzero count
+        list[kHWin + 1 - t_seg + p_seg++] = h;
+      } else {
+        h.cs = p_ent;
+        p_ent += cntq[q];
+        list[p_coo++] = h;
       }
     }
     if (tid == 0) list[t_coo].cs = t_ent;  // sentinel: end of the COO stream
     __syncthreads();
 
-    // ---- CSR phase: this warp's rows of every CSR block of the window
-    if (ra < rb) {
-      for (int i = 0; i < t_csr; ++i) {
-        const HBlk h = list[kHWin + 1 - t_csr + i];
-        const uint32_t* rp = row_ptr + h.off;
-        const int64_t lo = (int64_t)h.bp + __ldg(rp + ra), hi = (int64_t)h.bp + __ldg(rp + rb);
-        if (lo >= hi) continue;
-        hcsr_csr_rows<V, X, SA, MIX, VEC>(rp, h.bp, ra, rb, lo, hi, nz, col_idx, values, x + (int64_t)h.j * C, acc,
-                                          table, mgrp, lane, pf, pl);
+    // ---- row-range phase: this warp's rows of every CSR block and large
+    // COO block of the window, in block order.  A large COO block's rows
+    // ascend (the builder writes them so): the warp finds its nonzeros
+    // [first row >= ra, first row >= rb) by search and checks, on the way,
+    // that they ascend and lie in [ra, rb); a CTA whose warps met anything
+    // else redoes its block row with every COO block in the COO stream.
+    for (int i = 0; i < t_seg; ++i) {
+      const HBlk h = list[kHWin + 1 - t_seg + i];
+      const uint32_t* rp = row_ptr + h.off;
+      if (h.cs < 0) {
+        if (ra >= rb) continue;
+        hcsr_csr_rows<V, X, SA, MIX, VEC>(rp, h.bp, ra, rb, nz, col_idx, values, x + (int64_t)h.j * C, acc, table,
+                                          mgrp, lane, pf, pl);
+      } else {
+        const int cnt = h.cs;
+        const int klo = warp == 0 ? 0 : hcsr_lower_bound(rp, cnt, (uint32_t)ra, lane);
+        const int khi = warp == kHW - 1 ? cnt : hcsr_lower_bound(rp, cnt, (uint32_t)rb, lane);
+        if (klo > khi) {
+          if (lane == 0) s_bad = 1;
+          continue;
+        }
+        if (klo == khi) continue;
+        if (hcsr_seg_rows<V, X, SA, MIX, VEC, true>(rp, h.bp, ra, rb, (int64_t)h.bp + klo, (int64_t)h.bp + khi, nz,
+                                                    col_idx, values, x + (int64_t)h.j * C, acc, table, mgrp, lane,
+                                                    pf, pl))
+          s_bad = 1;
       }
     }
 
@@ -523,7 +773,14 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
     }
     __syncthreads();
   }
+  if (!big_ok || !s_bad) break;
+  // rows of a large COO block out of order: start over, all COO blocks
+  // through the COO stream
+  big_ok = false;
   __syncthreads();
+  for (int li = tid; li < rows; li += kHT) acc[li] = SA(0);
+  __syncthreads();
+  }
   for (int li = tid; li < rows; li += kHT) {
     const X o = (X)acc[li];
     X* yp = y + r0 + li;

@@ -15,25 +15,18 @@
 // Orders come from stable CUB radix sorts (column density, dense entries by
 // segment, rows by dense count, and per segment rows by (chunk, count)), so
 // the result does not depend on scheduling; counts use integer atomics.
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <cstring>
 #include <vector>
 
+#include "devsort.cuh"
 #include "rvvla_internal.cuh"
 #include "scan.cuh"
 
 namespace rvvla {
 namespace {
 
-inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
-
-int bits_for(uint64_t v) {
-  int b = 1;
-  while (b < 64 && (v >> b) != 0) ++b;
-  return b;
-}
+inline unsigned nblk(int64_t n) { return grid_for(n); }
 
 __global__ void lav_col_count_kernel(int64_t nz, const int* __restrict__ Col, int* __restrict__ cnt) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -239,17 +232,6 @@ __global__ void lav_long_chunks_kernel(int64_t cc, int64_t nseg, const int* __re
 __global__ void lav_i64_to_i32_kernel(int64_t n, const int64_t* __restrict__ in, int* __restrict__ out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (int)in[i];
-}
-
-template <class K, class V>
-int radix_sort_pairs(const K* kin, K* kout, const V* vin, V* vout, int64_t n, int end_bit, cudaStream_t st) {
-  if (n <= 0) return RVVLA_OK;
-  size_t tb = 0;
-  RVVLA_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit, st));
-  Scratch tmp;
-  RVVLA_CUDA(tmp.alloc(tb, st));
-  RVVLA_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, kin, kout, vin, vout, (int)n, 0, end_bit, st));
-  return RVVLA_OK;
 }
 
 template <class T>

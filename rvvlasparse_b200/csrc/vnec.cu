@@ -24,7 +24,6 @@
 
 #include "crs_merge.cuh"
 #include "rvvla_internal.cuh"
-#include "vnec_build.h"
 
 namespace rvvla {
 namespace {
@@ -219,54 +218,26 @@ int vnec_spmv_impl(const rvvla_vnec* A, X alpha, const X* x, X beta, X* y, cudaS
   return RVVLA_OK;
 }
 
+}  // namespace
+
+// vnec_build.cu
 template <class T>
-int upload(const std::vector<T>& v, T** dst, cudaStream_t st) {
-  RVVLA_CUDA(cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)));
-  if (!v.empty()) RVVLA_CUDA(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-  return RVVLA_OK;
-}
+int vnec_build_gpu(const rvvla_crs* src, int64_t NT, int force, int nL, double thr, rvvla_vnec_owned* out,
+                   cudaStream_t st);
+
+namespace {
 
 template <class T>
 int vnec_build_typed(const rvvla_crs* src, int64_t NT, int variant, rvvla_vnec_owned* out, cudaStream_t st) {
   const int64_t m = src->m, nz = src->nz;
-  std::vector<int> Rst((size_t)m + 1), Col((size_t)nz);
-  std::vector<T> Val((size_t)nz);
-  RVVLA_CUDA(cudaMemcpyAsync(Rst.data(), src->Rst, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
-  if (nz) {
-    RVVLA_CUDA(cudaMemcpyAsync(Col.data(), src->Col, nz * sizeof(int), cudaMemcpyDeviceToHost, st));
-    RVVLA_CUDA(cudaMemcpyAsync(Val.data(), src->Val, nz * sizeof(T), cudaMemcpyDeviceToHost, st));
-  }
-  RVVLA_CUDA(cudaStreamSynchronize(st));
+  if (m > 0 && (!src->Rst || (nz > 0 && (!src->Col || !src->Val))))
+    return fail(RVVLA_ERR_INVALID_ARG, "vnec_build: null array");
   const int nL = sizeof(T) == 4 ? 16 : 8;  // nLanes_f32 / nLanes_f64 (SpB_mxv_VNEC.h:22-23)
   const double thr = sizeof(T) == 4 ? 0.437 : 0.477;
-  VnecHost<T> H;
-  vnec_build_host<T>(Rst.data(), Col.data(), Val.data(), m, src->n, nz, NT, variant, nL, thr, H);
   rvvla_vnec& h = out->h;
-  h.m = m; h.n = src->n; h.nz = nz; h.NUM_THREADS_VNEC = (int32_t)NT; h.nLanes = nL; h.vnec_t = H.variant;
-  h.IRD_mat = H.ird; h.max_nec = H.max_nec;
-  int rc = 0;
-  if ((rc = upload(Rst, &out->ptr, st)) || (rc = upload(Col, &out->indices, st)) ||
-      (rc = upload(Val, reinterpret_cast<T**>(&out->val), st)) || (rc = upload(H.tcs, &out->thread_coord_start, st)) ||
-      (rc = upload(H.tce, &out->thread_coord_end, st)))
-    return rc;
-  if (H.variant == 0) {
-    if ((rc = upload(H.ecr, &out->ecr_indices, st)) || (rc = upload(H.nec, &out->NEC_NUM, st)) ||
-        (rc = upload(H.uxp, &out->use_x_ptr, st)) || (rc = upload(H.ux, &out->use_x_indices, st)) ||
-        (rc = upload(H.vrp, &out->v_row_ptr, st)) || (rc = upload(H.cs, &out->col_start, st)) ||
-        (rc = upload(H.va, reinterpret_cast<T**>(&out->val_align), st)))
-      return rc;
-    h.ngroups = (int64_t)H.cs.size();
-  } else if (H.variant == 1) {
-    if ((rc = upload(H.nec, &out->NEC_NUM, st)) || (rc = upload(H.uxp, &out->use_x_ptr, st)) ||
-        (rc = upload(H.ux, &out->use_x_indices, st)) || (rc = upload(H.tasks, &out->tasks, st)) ||
-        (rc = upload(H.ts, &out->task_start, st)) || (rc = upload(H.te, &out->task_end, st)) ||
-        (rc = upload(H.spv, &out->spvv_len, st)) || (rc = upload(H.rb, &out->row_begin, st)) ||
-        (rc = upload(H.re, &out->row_end, st)) || (rc = upload(H.rc, &out->reorder_col, st)) ||
-        (rc = upload(H.rv, reinterpret_cast<T**>(&out->reorder_nnz), st)))
-      return rc;
-    h.ntasks = (int64_t)H.tasks.size();
-    h.nreorder = (int64_t)H.rc.size();
-  }
+  h.m = m; h.n = src->n; h.nz = nz; h.NUM_THREADS_VNEC = (int32_t)NT; h.nLanes = nL;
+  int rc = vnec_build_gpu<T>(src, NT, variant, nL, thr, out, st);
+  if (rc) return rc;
   h.ptr = out->ptr; h.indices = out->indices; h.val = out->val;
   h.thread_coord_start = out->thread_coord_start; h.thread_coord_end = out->thread_coord_end;
   h.ecr_indices = out->ecr_indices; h.NEC_NUM = out->NEC_NUM; h.use_x_ptr = out->use_x_ptr;
@@ -274,7 +245,7 @@ int vnec_build_typed(const rvvla_crs* src, int64_t NT, int variant, rvvla_vnec_o
   h.val_align = out->val_align; h.tasks = out->tasks; h.task_start = out->task_start; h.task_end = out->task_end;
   h.spvv_len = out->spvv_len; h.row_begin = out->row_begin; h.row_end = out->row_end;
   h.reorder_col = out->reorder_col; h.reorder_nnz = out->reorder_nnz;
-  if (H.variant == 2 && nz > 0) {
+  if (h.vnec_t == 2 && nz > 0) {
     // L: analyse the source CRS once for the CRS lane-run kernel
     const int dt = sizeof(T) == 8 ? RVVLA_F64 : RVVLA_F32;
     const int64_t plen = rvvla_crs_plan_len(m, nz, dt);

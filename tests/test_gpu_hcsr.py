@@ -111,6 +111,43 @@ def test_hcsr_tall_block_rows(R_):
     assert np.array_equal(a, run(H, 1.0, x, 2.0, y0))
 
 
+@pytest.mark.parametrize("how", ["reversed", "ends_swapped"])
+def test_hcsr_coo_rows_out_of_order(how):
+    """COO blocks whose nonzeros are not in row order (a hand-made HCSR; the
+    builder writes them in order): the large ones, which the kernel splits
+    among its warps by row, fall back to the COO stream and the product stays
+    within the fp64 bar.  Every COO block reversed, or only its first and
+    last nonzeros swapped."""
+    m, n, Rst, Col, Val = W.powerlaw(300000, seed=12)
+    x, y0 = W.vector(n, 1), W.vector(m, 2)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.5, y0)
+    H = hcsr(m, n, Rst, Col, Val, torch.float64, R=3000, C=1 << 16, p=50.0)
+    ordered = run(H, 1.0, x, 0.5, y0)
+    h = H.to_host()
+    bp = h["block_ptr"].astype(np.int64)
+    ro = h["row_offset"].view(np.uint32)
+    rows, cols, vals = h["row_ptr"].copy(), h["col_idx"].copy(), h["values"].copy()
+    n_large = 0
+    for b in range(len(bp) - 1):
+        lo, hi = int(bp[b]), int(bp[b + 1])
+        if hi - lo < 2 or (ro[b] >> 30) == 1:
+            continue
+        off = int(ro[b] & 0x3FFFFFFF)
+        if rows[off] == rows[off + hi - lo - 1]:
+            continue
+        sel = np.arange(hi - lo)[::-1] if how == "reversed" else np.r_[hi - lo - 1, 1:hi - lo - 1, 0]
+        rows[off:off + hi - lo] = rows[off:off + hi - lo][sel]
+        cols[lo:hi] = cols[lo:hi][sel]
+        vals[lo:hi] = vals[lo:hi][sel]
+        n_large += hi - lo >= 2048
+    assert n_large > 10
+    H.row_ptr, H.col_idx, H.values = dev(rows), dev(cols), dev(vals)
+    a = run(H, 1.0, x, 0.5, y0)
+    assert O.normwise_relerr(a, yref) < 1e-12
+    assert O.normwise_relerr(ordered, yref) < 1e-12
+    assert np.array_equal(a, run(H, 1.0, x, 0.5, y0))
+
+
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 def test_hcsr_unaligned_arrays(dt):
     """values / col_idx not 16-byte aligned (scalar loads) give the same
