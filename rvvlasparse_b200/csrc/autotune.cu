@@ -6,7 +6,8 @@
 // caller's CRS, one product is run untimed, then `iters` products are timed
 // with CUDA events on `stream` and the best time kept; the build is freed
 // before the next candidate.  Candidates per format:
-//   HCSR   square blocks R = C in {512, 1024, 2000, 4000, 8192}, p = 2;
+//   HCSR   square blocks R = C in {512, 1024, 2000, 4000, 8192} and
+//          R in {1000, 2000, 4000} with C = 65536, p = 2;
 //   SELL   C = 32 (a warp per slice), sigma in {32, 256, 1024, 8192};
 //   CSR5   omega = 32, sigma in {8, 16, 24, 32};
 //   LAV    SIMD_Lanes 8, T 0.2, segment_len in {40000, n/4, n};
@@ -36,6 +37,13 @@ std::vector<rvvla_tune_params> candidates(int fmt, const rvvla_crs* A) {
       for (int64_t b : {512, 1024, 2000, 4000, 8192}) {
         auto p = blank();
         p.R = p.C = b;
+        out.push_back(p);
+      }
+      // the widest blocks the uint16 columns allow: fewer, larger blocks
+      for (int64_t r : {1000, 2000, 4000}) {
+        auto p = blank();
+        p.R = r;
+        p.C = 65536;
         out.push_back(p);
       }
       break;

@@ -70,8 +70,9 @@ constexpr int kHT = 32 * kHW;              // threads per CTA
 constexpr int kHMinBlocks = 2;             // resident CTAs per SM the registers are sized for
 constexpr int kHWLog = kHW == 8 ? 3 : 4;
 static_assert(kHW == 8 || kHW == 16, "8 or 16 row owners");
-constexpr int kHWin = 4 * kHT;             // block columns per window (4 per thread)
-constexpr int kHRound = 2048;              // COO nonzeros per round
+constexpr int kHPer = 1;                   // block columns per thread in a window
+constexpr int kHWin = kHPer * kHT;         // block columns per window
+constexpr int kHRound = 1024;              // COO nonzeros per round
 constexpr int kHU = kHRound / (kHW * 32);  // sub-steps of 32 per warp and round
 constexpr int kHSlots = 2048 / kHW;        // per-warp row slots of the COO apply (power of two)
 constexpr int kHBig = 1024;                // COO blocks of at least this many nonzeros take the row-range path
@@ -556,16 +557,16 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
   for (;;) {
   for (int64_t jw = 0; jw < b_n; jw += kHWin) {
     const int nb = (int)(b_n - jw < kHWin ? b_n - jw : kHWin);
-    // ---- compact the window's non-empty blocks (4 consecutive per thread):
+    // ---- compact the window's non-empty blocks (kHPer consecutive per thread):
     // CSR blocks and COO blocks of >= kHBig nonzeros form the row-range list
     // (block order, from the back of `list`), the smaller COO blocks the COO
     // stream (from the front, with a sentinel)
-    int bpq[4], cntq[4];
-    uint32_t roq[4];
-    int kindq[4];  // 0 none, 1 CSR, 2 large COO, 3 small COO
+    int bpq[kHPer], cntq[kHPer];
+    uint32_t roq[kHPer];
+    int kindq[kHPer];  // 0 none, 1 CSR, 2 large COO, 3 small COO
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int jj = 4 * tid + q;
+    for (int q = 0; q < kHPer; ++q) {
+      const int jj = kHPer * tid + q;
       bpq[q] = 0;
       cntq[q] = 0;
       roq[q] = 0u;
@@ -580,7 +581,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
     }
     int n_seg = 0, n_coo = 0, n_ent = 0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < kHPer; ++q) {
       if (kindq[q] == 1 || kindq[q] == 2) ++n_seg;
       if (kindq[q] == 3) {
         ++n_coo;
@@ -590,12 +591,12 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
     int p_seg, p_coo, p_ent, t_seg, t_coo, t_ent;
     hcsr_scan3(n_seg, n_coo, n_ent, p_seg, p_coo, p_ent, t_seg, t_coo, t_ent, s_w);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < kHPer; ++q) {
       if (kindq[q] == 0) continue;
       HBlk h;
       h.bp = bpq[q];
       h.off = roq[q] & kHKindMask;
-      h.j = (int)(jw + 4 * tid + q);
+      h.j = (int)(jw + kHPer * tid + q);
       if (kindq[q] == 1 || kindq[q] == 2) {
         h.cs = kindq[q] == 1 ? -1 : cntq[q];  // a large COO block keeps its nonzero count
         list[kHWin + 1 - t_seg + p_seg++] = h;
@@ -809,7 +810,10 @@ template <class V, class X, class SA, bool MIX, bool VEC, bool GACC>
 int hcsr_launch(const rvvla_hcsr* A, X alpha, const X* x, X beta, X* y, SA* gacc, size_t smem, cudaStream_t st) {
   auto kern = hcsr_spmv_kernel<V, X, SA, MIX, VEC, GACC>;
   RVVLA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  prefer_shared(kern);
+  // shared memory for kHMinBlocks CTAs, the rest of the SM's 256 KB as L1
+  // (the gathers of x hit there)
+  const int carve = (int)std::min<size_t>(100, (kHMinBlocks * (smem + 1024) * 100 + kHSmemMax - 1) / kHSmemMax);
+  RVVLA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
   kern<<<(unsigned)A->b_m, kHT, smem, st>>>(A->R, A->C, A->m, A->nz, A->b_n, A->block_ptr, A->row_offset,
                                             A->row_ptr, A->col_idx, (const V*)A->values, x, y, alpha, beta, gacc);
   RVVLA_LAUNCHED("hcsr_spmv_kernel");
