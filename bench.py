@@ -72,9 +72,12 @@ def workload(name: str, n: int, cpu_only: bool = False):
 
 def config_for(args, m: int, nnz: int, case_names: list, world: int) -> dict:
     """The workload description, identical in both arms."""
-    return {"workload": f"{args.workload} n={m} nnz={nnz}", "cases": case_names, "alpha": 1.0, "beta": 0.0,
-            "parallelism": f"replicas{world}",
-            "l2": "matrix arrays larger than the 126 MB L2 (streamed from HBM every step); x L2-resident"}
+    cfg = {"workload": f"{args.workload} n={m} nnz={nnz}", "cases": case_names, "alpha": 1.0, "beta": 0.0,
+           "parallelism": f"replicas{world}",
+           "l2": "matrix arrays larger than the 126 MB L2 (streamed from HBM every step); x L2-resident"}
+    if getattr(args, "params", ""):
+        cfg["params"] = parse_params(args.params)
+    return cfg
 
 
 # formats the reference implements in C++ (src/scalar, built unmodified into
@@ -163,10 +166,23 @@ def cvr_bytes(Cv, vb, xb):
 MIXED = ("crs", "hcsr", "csr5", "sell")
 
 
-def build_cases(m, n, Rst, Col, Val, formats, precs):
+def parse_params(text: str) -> dict:
+    """--params "hcsr:R=2000,C=65536;csr5:sigma=24" -> {fmt: {key: number}}."""
+    out = {}
+    for part in filter(None, (t.strip() for t in text.split(";"))):
+        fmt, _, kv = part.partition(":")
+        d = out.setdefault(fmt.strip(), {})
+        for item in filter(None, kv.split(",")):
+            k, _, v = item.partition("=")
+            d[k.strip()] = float(v) if "." in v else int(v)
+    return out
+
+
+def build_cases(m, n, Rst, Col, Val, formats, precs, overrides=None):
     """One Case per (format, precision).  Precisions: f64, f32, mixed (fp32
     values, compensated fp32 sums, fp64 carry merges) and mixed_bf16 (the
-    same with bf16 values); the mixed forms exist for CRS, HCSR, CSR5, SELL."""
+    same with bf16 values); the mixed forms exist for CRS, HCSR, CSR5, SELL.
+    overrides: {fmt: convertParams entries} over the defaults below."""
     import torch
 
     import rvvlasparse_b200 as R
@@ -193,6 +209,7 @@ def build_cases(m, n, Rst, Col, Val, formats, precs):
         "cvr": (R.spMtxCVR, {}, cvr_bytes)}
     for fmt in formats:
         cls, params, nbytes = spec[fmt]
+        params = {**params, **(overrides or {}).get(fmt, {})}
         built = {}
         for p in precs:
             if p.startswith("mixed") and fmt not in MIXED:
@@ -299,7 +316,8 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     lib = R.load()
     m, n, Rst, Col, Val = workload(args.workload, args.n)
-    cases = build_cases(m, n, Rst, Col, Val, args.formats.split(","), args.precisions.split(","))
+    cases = build_cases(m, n, Rst, Col, Val, args.formats.split(","), args.precisions.split(","),
+                        parse_params(args.params))
     stream = torch.cuda.current_stream()
     for _ in range(max(args.warmup, 3)):
         for c in cases:
@@ -934,6 +952,8 @@ def main():
                          "instead of a replica of every case per rank")
     ap.add_argument("--exchange", default="halo", choices=["halo", "allgather"],
                     help="x exchange of --sharded")
+    ap.add_argument("--params", default="",
+                    help='convertParams per format over the defaults, e.g. "hcsr:R=2000,C=65536;csr5:sigma=24"')
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the drop-in end-to-end leg (a child process; for profiling runs)")
     ap.add_argument("--no-forms", action="store_true",

@@ -218,7 +218,9 @@ __device__ __forceinline__ void hcsr_add(SA* acc, int r, T v) {
 // the lanes' slots through a per-warp table; each lane sums its products
 // split at the marks, and a reverse segmented scan adds the parts of rows
 // crossing lanes.  When no lane holds two row starts (rows of 8 or more
-// nonzeros), a lane's sums take the branch-free split at its one mark.
+// nonzeros), a lane's sums take the short split at its one mark.  The
+// columns of a chunk are loaded one chunk ahead, so that its x gathers leave
+// together with its value loads.
 template <class V, class X, class SA, bool MIX, bool VEC>
 __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t nz,
                                               const uint16_t* __restrict__ col_idx, const V* __restrict__ values,
@@ -245,10 +247,20 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
   ldwin(wb, s_c, e_c);
   ldwin(wb + 32, s_n, e_n);
   int open_row = -1;
-  for (uint32_t c = lo & ~7u; c < hi; c += kHChunk) {
+  // the lane's 8 columns of the next chunk, loaded one chunk ahead, so that
+  // a chunk's x gathers leave together with its value loads
+  const uint32_t c0 = lo & ~7u;
+  int4 cn = make_int4(0, 0, 0, 0);
+  if (VEC && c0 + kHLane * lane + kHLane <= lim) cn = ld_v4_l1(cb + c0 + kHLane * lane, pf);
+  for (uint32_t c = c0; c < hi; c += kHChunk) {
     const uint32_t a = c + kHLane * lane;
     const uint32_t fv = lo > a ? lo - a : 0u;  // the lane's slots in [fv, lv) lie in [lo, hi)
     const uint32_t lv = hi > a ? hi - a : 0u;
+    const int4 cw = cn;
+    if (VEC) {
+      const uint32_t an = a + kHChunk;
+      cn = c + kHChunk < hi && an + kHLane <= lim ? ld_v4_l1(cb + an, pf) : make_int4(0, 0, 0, 0);
+    }
     // ---- loads and products
     PT p[kHLane];
     {
@@ -256,7 +268,12 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
       uint32_t cc[kHLane];
       if (VEC && a + kHLane <= lim) {
         hcsr_vals(vb + a, vv, pf);
-        hcsr_cols(cb + a, cc, pf);
+        const uint32_t w[4] = {(uint32_t)cw.x, (uint32_t)cw.y, (uint32_t)cw.z, (uint32_t)cw.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          cc[2 * q] = w[q] & 0xFFFFu;
+          cc[2 * q + 1] = w[q] >> 16;
+        }
       } else {
 #pragma unroll
         for (int i = 0; i < kHLane; ++i) {
@@ -300,12 +317,17 @@ __device__ __forceinline__ void hcsr_csr_rows(const uint32_t* __restrict__ rp, i
       const int m = mb ? __ffs(mb) - 1 : kHLane;
 #pragma unroll
       for (int i = 0; i < kHLane; ++i) {
-        if (i < m) acc_add(lead, p[i]);
-        else acc_add(sum, p[i]);
+        if (i == m) {
+          lead = sum;
+          acc_zero(sum);
+        }
+        acc_add(sum, p[i]);
       }
       if (mb) {
         nf = 1;
         rcur = table[kHLane * lane + m];
+      } else {
+        lead = sum;
       }
     } else {
 #pragma unroll
