@@ -32,7 +32,7 @@
 //     rows out of order there starts its block row over with every COO block
 //     in the COO phase;
 //   * COO phase: the window's other COO nonzeros (in block order) are cut
-//     into rounds of 2048; every warp computes 128 products in stream order
+//     into rounds of 1024; every warp computes 64 products in stream order
 //     (the block of each nonzero from the compacted list: a warp-wide OR of
 //     the next block starts and a popcount), writes (row, product, owner) to
 //     shared memory — a run of one row inside one block summed first, by a
@@ -46,8 +46,10 @@
 //     lowest pending lane of each row per round).
 // The next round's loads are issued before the current round is applied.
 // Per row, the sum is: row-range pieces of window 0 in block order, COO
-// products of window 0 in stream order, then window 1, ...; y = alpha*acc + beta*y at the
-// end (y is not read when beta == 0).
+// products of window 0 in stream order, then window 1, ...; y = alpha*acc +
+// beta*y at the end (y is not read when beta == 0).  Shared memory is sized
+// for two CTAs per SM and the carveout asks for no more, so that the rest of
+// the SM's 256 KB serves as L1 for the gathers of x.
 //
 // Mixed forms: lane sums of the CSR phase in compensated fp32 (two-sum), COO
 // products in fp32; the block-row accumulator, where pieces of different
@@ -721,14 +723,18 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
           }
           // runs of one row inside one block (consecutive lanes) are summed
           // here; only the run's last lane is handed on
+          // (cont: this lane continues the previous lane's run; most
+          // sub-steps have none, and skip the scan)
           const uint32_t prow = __shfl_up_sync(0xffffffffu, r.row, 1);
           const int64_t pxo = __shfl_up_sync(0xffffffffu, r.xoff, 1);
-          const bool head = lane == 0 || !r.ok || prow != r.row || pxo != r.xoff;
-          const P run = warp_seg_scan(pv, head, lane);
-          const uint32_t nrow = __shfl_down_sync(0xffffffffu, r.row, 1);
-          const int64_t nxo = __shfl_down_sync(0xffffffffu, r.xoff, 1);
-          const bool nok = __shfl_down_sync(0xffffffffu, r.ok, 1);
-          const bool tail = r.ok && (lane == 31 || !nok || nrow != r.row || nxo != r.xoff);
+          const bool cont = lane > 0 && r.ok && prow == r.row && pxo == r.xoff;
+          P run = pv;
+          bool tail = r.ok;
+          if (__any_sync(0xffffffffu, cont)) {
+            run = warp_seg_scan(pv, !cont, lane);
+            const bool ncont = __shfl_down_sync(0xffffffffu, cont, 1);
+            tail = r.ok && (lane == 31 || !ncont);
+          }
           s_prod[i] = run;
           s_row[i] = r.row;
           s_own[i] = (uint8_t)(tail ? hcsr_coo_owner(r.row) : 0xFFu);
