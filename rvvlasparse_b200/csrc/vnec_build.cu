@@ -83,13 +83,29 @@ __global__ void vnec_row_of_kernel(int64_t m, const int* __restrict__ Rst, int* 
   for (int k = Rst[r]; k < Rst[r + 1]; ++k) row_of[k] = (int)r;
 }
 
+// The keys are sorted, so a warp's keys fall in a few runs of one piece:
+// one atomic per run (the last lane of the run adds the run's distinct keys).
 __global__ void vnec_uniq_kernel(int64_t n, const uint64_t* __restrict__ key, int64_t* __restrict__ flag,
                                  int* __restrict__ nec) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const bool u = p == 0 || key[p] != key[p - 1];
-  flag[p] = u ? 1 : 0;
-  if (u) atomicAdd(nec + (key[p] >> 32), 1);
+  const int lane = threadIdx.x & 31;
+  const bool valid = p < n;
+  const uint64_t k = valid ? key[p] : 0;
+  const bool u = valid && (p == 0 || k != key[p - 1]);
+  if (valid) flag[p] = u ? 1 : 0;
+  const uint32_t piece = (uint32_t)(k >> 32);
+  const uint32_t np = __shfl_down_sync(0xffffffffu, piece, 1);
+  const bool nvalid = __shfl_down_sync(0xffffffffu, valid, 1);
+  const bool last = valid && (lane == 31 || !nvalid || np != piece);
+  const unsigned um = __ballot_sync(0xffffffffu, u);
+  const unsigned lm = __ballot_sync(0xffffffffu, last);
+  if (last) {
+    const unsigned below = lm & ((1u << lane) - 1u);
+    const int start = below ? 32 - __clz(below) : 0;  // first lane of this run
+    const unsigned run = (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u)) & ~((1u << start) - 1u);
+    const int cnt = __popc(um & run);
+    if (cnt) atomicAdd(nec + piece, cnt);
+  }
 }
 
 // ranks and the distinct column lists: excl = exclusive scan of the flags
