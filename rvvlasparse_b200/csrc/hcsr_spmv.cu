@@ -76,6 +76,7 @@ constexpr int kHPer = 1;                   // block columns per thread in a wind
 constexpr int kHWin = kHPer * kHT;         // block columns per window
 constexpr int kHRound = 1024;              // COO nonzeros per round
 constexpr int kHU = kHRound / (kHW * 32);  // sub-steps of 32 per warp and round
+constexpr int kHStages = 2;                // COO stage buffers (round t fills t % kHStages)
 constexpr int kHSlots = 2048 / kHW;        // per-warp row slots of the COO apply (power of two)
 constexpr int kHBig = 1024;                // COO blocks of at least this many nonzeros take the row-range path
 constexpr int kHLane = 8;                  // CSR nonzeros per lane and chunk
@@ -103,9 +104,9 @@ struct HLayout {
     acc = 0;
     list = hal16((size_t)racc * sizeof(SA));
     prod = list + hal16((size_t)(kHWin + 1) * sizeof(HBlk));
-    row = prod + hal16((size_t)kHRound * sizeof(P));
-    own = row + (size_t)kHRound * 4;
-    wscr = own + hal16((size_t)kHRound);
+    row = prod + hal16((size_t)kHStages * kHRound * sizeof(P));
+    own = row + (size_t)kHStages * kHRound * 4;
+    wscr = own + hal16((size_t)kHStages * kHRound);
     mgrp = wscr + (size_t)kHW * kHWscr;
     slot = mgrp + (size_t)kHW * 32 * 4;
     total = slot + (size_t)kHW * kHSlots * 4;
@@ -558,9 +559,9 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
   const int rows = (int)min(R, m - r0);
   SA* acc = GACC ? gacc + r0 : reinterpret_cast<SA*>(smem + L.acc);
   HBlk* list = reinterpret_cast<HBlk*>(smem + L.list);
-  P* s_prod = reinterpret_cast<P*>(smem + L.prod);
-  uint32_t* s_row = reinterpret_cast<uint32_t*>(smem + L.row);
-  uint8_t* s_own = smem + L.own;
+  P* s_prod0 = reinterpret_cast<P*>(smem + L.prod);
+  uint32_t* s_row0 = reinterpret_cast<uint32_t*>(smem + L.row);
+  uint8_t* s_own0 = smem + L.own;
   int* table = reinterpret_cast<int*>(smem + L.wscr + (size_t)warp * kHWscr);          // CSR phase
   uint16_t* olist = reinterpret_cast<uint16_t*>(smem + L.wscr + (size_t)warp * kHWscr);  // COO phase
   uint32_t* mgrp = reinterpret_cast<uint32_t*>(smem + L.mgrp) + warp * 32;
@@ -708,6 +709,11 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
       };
       coo_load(0);
       for (int t = 0; t < nrounds; ++t) {
+        // this round's stage buffer: with two, round t + 1 is produced while
+        // slower warps still apply round t, and one barrier per round does
+        P* const s_prod = s_prod0 + (t % kHStages) * kHRound;
+        uint32_t* const s_row = s_row0 + (t % kHStages) * kHRound;
+        uint8_t* const s_own = s_own0 + (t % kHStages) * kHRound;
         // products of this round into shared memory, in stream order
         X xv[kHU];
 #pragma unroll
@@ -797,7 +803,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
             }
           }
         }
-        __syncthreads();
+        if (kHStages == 1) __syncthreads();
       }
     }
     __syncthreads();
