@@ -661,6 +661,18 @@ int rvvla_cg_f64(const rvvla_crs* A, const double* b, double* x, int64_t max_ite
                  int64_t check_every, int64_t* iters, double* rel_res, void* stream);
 int rvvla_cg_f32(const rvvla_crs* A, const float* b, float* x, int64_t max_iter, double rtol,
                  int64_t check_every, int64_t* iters, double* rel_res, void* stream);
+/* BiCGStab (van der Vorst) for a general square A, unpreconditioned (no
+ * reference counterpart: a caller of the SpMV path).  Same A, x, b, limits
+ * and check schedule as rvvla_cg_*; per iteration two CRS products
+ * (v = A p, t = A s), the dots r^.v, t.s, t.t, r^.r and r.r reduced in a
+ * fixed order, and three fused vector passes, scalars on the device.
+ * *breakdown = 1 when it stopped unconverged because r^.r, r^.v or t.t
+ * became exactly zero (RVVLA_OK either way).  Scratch: 6 vectors of n plus
+ * partials, stream-ordered.  Bitwise reproducible. */
+int rvvla_bicgstab_f64(const rvvla_crs* A, const double* b, double* x, int64_t max_iter, double rtol,
+                       int64_t check_every, int64_t* iters, double* rel_res, int* breakdown, void* stream);
+int rvvla_bicgstab_f32(const rvvla_crs* A, const float* b, float* x, int64_t max_iter, double rtol,
+                       int64_t check_every, int64_t* iters, double* rel_res, int* breakdown, void* stream);
 /* y = A x and *dot = x^T A x (a device scalar) in one pass over A: the
  * building block of the solver for other Krylov methods.  A square with an
  * rvvla_crs_analyze plan (or without nonzeros: y = 0, *dot = 0); the dot

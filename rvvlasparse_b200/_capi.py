@@ -273,6 +273,8 @@ def load():
     _proto(lib, "rvvla_gen_vector", None, i64, u64, cint, dbl, dbl, vp)
     _proto(lib, "rvvla_cg_f64", cint, P(rvvla_crs), vp, vp, i64, dbl, i64, P(i64), P(dbl), vp)
     _proto(lib, "rvvla_cg_f32", cint, P(rvvla_crs), vp, vp, i64, dbl, i64, P(i64), P(dbl), vp)
+    _proto(lib, "rvvla_bicgstab_f64", cint, P(rvvla_crs), vp, vp, i64, dbl, i64, P(i64), P(dbl), P(cint), vp)
+    _proto(lib, "rvvla_bicgstab_f32", cint, P(rvvla_crs), vp, vp, i64, dbl, i64, P(i64), P(dbl), P(cint), vp)
     _proto(lib, "rvvla_crs_spmv_dot_f64", cint, P(rvvla_crs), vp, vp, vp, vp)
     _proto(lib, "rvvla_crs_spmv_dot_f32", cint, P(rvvla_crs), vp, vp, vp, vp)
     cp = C.c_char_p

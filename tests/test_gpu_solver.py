@@ -121,3 +121,102 @@ def test_spmv_dot_fused(dt):
         assert abs(float(d.item()) - dref) / abs(dref) < (1e-11 if dt == np.float64 else 1e-4)
         y2, d2 = S.spmv_dot(A, x)
         assert torch.equal(y, y2) and torch.equal(d, d2)
+
+
+# ---------------------------------------------------------------- BiCGStab
+
+def numpy_bicgstab(A, b, rtol, max_iter):
+    """Unpreconditioned BiCGStab with the recurrences of rvvla_bicgstab_*."""
+    x = np.zeros_like(b)
+    r = b - A @ x
+    rh = r.copy()
+    p = np.zeros_like(b)
+    v = np.zeros_like(b)
+    rho, alpha, omega, beta = rh @ r, 1.0, 1.0, 0.0
+    bb = b @ b
+    rr = r @ r
+    it = 0
+    while np.sqrt(rr / bb) > rtol and it < max_iter:
+        p = r + beta * (p - omega * v)
+        v = A @ p
+        alpha = rho / (rh @ v)
+        s = r - alpha * v
+        t = A @ s
+        omega = (t @ s) / (t @ t)
+        x += alpha * p + omega * s
+        r = s - omega * t
+        rho_new = rh @ r
+        beta = (rho_new / rho) * (alpha / omega)
+        rho = rho_new
+        rr = r @ r
+        it += 1
+    return x, it
+
+
+def convection_diffusion(g, c):
+    """5-point Laplacian plus a first-order convection term of strength c:
+    non-symmetric, diagonally dominant."""
+    e = np.ones(g)
+    T = sp.diags([-(1 + c) * e[:-1], 4 * e, -(1 - c) * e[:-1]], [-1, 0, 1])
+    I = sp.identity(g)
+    S1 = sp.diags([-e[:-1], -e[:-1]], [-1, 1])
+    A = (sp.kron(I, T) + sp.kron(S1, I)).tocsr()
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("g,c", [(48, 0.3), (160, 0.7)])
+def test_bicgstab_fp64_matches_direct_and_numpy(g, c):
+    As = convection_diffusion(g, c)
+    m = As.shape[0]
+    A = R.spMtxCRS.from_host(m, m, As.indptr.astype(np.int32), As.indices.astype(np.int32), As.data,
+                             dtype=torch.float64)
+    b = W.vector(m, 11)
+    x, it, rel, bd = S.bicgstab(A, torch.as_tensor(b).cuda(), rtol=1e-10, max_iter=5000, check_every=1)
+    xh = x.cpu().numpy()
+    assert not bd and rel <= 1e-10
+    assert np.linalg.norm(b - As @ xh) / np.linalg.norm(b) < 1e-9  # true residual
+    xd = spla.spsolve(As.tocsc(), b)
+    assert np.linalg.norm(xh - xd) / np.linalg.norm(xd) < 1e-7
+    _, it_np = numpy_bicgstab(As, b, 1e-10, 5000)
+    assert abs(it - it_np) <= 3
+    # bitwise reproducible; a later check only runs a few more iterations
+    x2, it2, _, _ = S.bicgstab(A, torch.as_tensor(b).cuda(), rtol=1e-10, max_iter=5000, check_every=1)
+    assert it2 == it and torch.equal(x, x2)
+    _, it10, rel10, _ = S.bicgstab(A, torch.as_tensor(b).cuda(), rtol=1e-10, max_iter=5000, check_every=10)
+    assert it <= it10 < it + 10 and rel10 <= 1e-10
+
+
+def test_bicgstab_fp32_and_limits():
+    As = convection_diffusion(64, 0.5)
+    m = As.shape[0]
+    Rst, Col = As.indptr.astype(np.int32), As.indices.astype(np.int32)
+    A32 = R.spMtxCRS.from_host(m, m, Rst, Col, As.data.astype(np.float32), dtype=torch.float32)
+    b = W.vector(m, 12)
+    x, it, rel, bd = S.bicgstab(A32, torch.as_tensor(b.astype(np.float32)).cuda(), rtol=1e-5, max_iter=2000)
+    assert not bd and rel <= 1e-5
+    xh = x.double().cpu().numpy()
+    assert np.linalg.norm(b - As @ xh) / np.linalg.norm(b) < 1e-4
+    # max_iter stops it; an exact initial guess needs no iteration
+    A64 = R.spMtxCRS.from_host(m, m, Rst, Col, As.data, dtype=torch.float64)
+    _, it3, rel3, _ = S.bicgstab(A64, torch.as_tensor(b).cuda(), rtol=1e-14, max_iter=3, check_every=2)
+    assert it3 == 3 and rel3 > 1e-14
+    xd = spla.spsolve(As.tocsc(), b)
+    _, it0, rel0, _ = S.bicgstab(A64, torch.as_tensor(b).cuda(), x0=torch.as_tensor(xd).cuda(), rtol=1e-8)
+    assert it0 == 0 and rel0 <= 1e-8
+
+
+def test_bicgstab_rejects_bad_arguments():
+    As = convection_diffusion(8, 0.1)
+    m = As.shape[0]
+    A = R.spMtxCRS.from_host(m, m, As.indptr.astype(np.int32), As.indices.astype(np.int32), As.data,
+                             dtype=torch.float64)
+    b = torch.ones(m, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        S.bicgstab(A, b[:-1])
+    with pytest.raises(ValueError):
+        S.bicgstab(A, b, check_every=0)
+    Rn = np.array([0, 1, 2], np.int32)
+    An = R.spMtxCRS.from_host(2, 3, Rn, np.array([0, 2], np.int32), np.ones(2), dtype=torch.float64)
+    with pytest.raises(ValueError):
+        S.bicgstab(An, torch.ones(2, dtype=torch.float64, device="cuda"))
