@@ -383,44 +383,29 @@ __device__ __forceinline__ int hcsr_lower_bound(const uint32_t* __restrict__ row
   return lo + __popc(__ballot_sync(0xffffffffu, less));
 }
 
-// Row-range phase of one warp for one block: the nonzeros [lo, hi)
-// (absolute) of the warp's rows [ra, rb).  CSR block (COO = false): row starts
-// come from rp (the block's row_ptr, block-relative) in windows of 32 rows.
-// COO block (COO = true): rp holds each nonzero's row (rp[k - bp]); a row
-// starts where the row differs from the previous nonzero's.  Returns true
-// (COO only) when a row descends or lies outside [ra, rb); such nonzeros are
-// left out.
-template <class V, class X, class SA, bool MIX, bool VEC, bool COO>
-__device__ __forceinline__ bool hcsr_seg_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t lo,
+// Row-range phase of one warp for one large COO block: the nonzeros
+// [lo, hi) (absolute) that hold the warp's rows [ra, rb), in chunks of 256 as
+// in hcsr_csr_rows.  rp holds each nonzero's row (rp[k - bp]); a row starts
+// where the row differs from the previous kept nonzero's.  Returns true when
+// a row descends or lies outside [ra, rb); such nonzeros are left out.
+template <class V, class X, class SA, bool MIX, bool VEC>
+__device__ __forceinline__ bool hcsr_coo_rows(const uint32_t* __restrict__ rp, int64_t bp, int ra, int rb, int64_t lo,
                                               int64_t hi, int64_t nz, const uint16_t* __restrict__ col_idx,
                                               const V* __restrict__ values, const X* __restrict__ xb, SA* acc,
-                                              int* table, uint32_t* mgrp, int lane, uint64_t pf, uint64_t pl) {
+                                              int lane, uint64_t pf, uint64_t pl) {
   using Ty = HTypes<V, X, SA, MIX>;
   using Ac = typename Ty::Ac;
   using PT = typename Ty::PT;
   using CT = SA;
-  // row window: lane l holds the starts of rows wb + l and wb + l + 1 (the
-  // next window is loaded one window ahead)
-  int wb = ra;
-  auto ldwin = [&](int base, uint32_t& s, uint32_t& e) {
-    const int r = base + lane;
-    s = r < rb ? __ldg(rp + r) : 0xFFFFFFFFu;
-    e = r < rb ? __ldg(rp + r + 1) : 0xFFFFFFFFu;
-  };
-  uint32_t s_c = 0, e_c = 0, s_n = 0, e_n = 0;
-  if constexpr (!COO) {
-    ldwin(wb, s_c, e_c);
-    ldwin(wb + 32, s_n, e_n);
-  }
-  uint32_t last_row = 0xFFFFFFFFu;   // COO: row of the last nonzero before the chunk
-  uint32_t last_kept = 0xFFFFFFFFu;  // COO: the same, of the kept nonzeros
+  uint32_t last_row = 0xFFFFFFFFu;   // row of the last nonzero before the chunk
+  uint32_t last_kept = 0xFFFFFFFFu;  // the same, of the kept nonzeros
   bool bad = false;
   int open_row = -1;
   for (int64_t c = lo & ~(int64_t)7; c < hi; c += kHChunk) {
     const int64_t a = c + kHLane * lane;
-    // ---- COO: rows (0xFFFFFFFF outside [lo, hi) and outside [ra, rb))
+    // ---- rows (0xFFFFFFFF outside [lo, hi) and outside [ra, rb))
     uint32_t rw[kHLane];
-    if constexpr (COO) {
+    {
 #pragma unroll
       for (int i = 0; i < kHLane; ++i) rw[i] = a + i >= lo && a + i < hi ? __ldg(rp + (a + i - bp)) : 0xFFFFFFFFu;
       uint32_t before = __shfl_up_sync(0xffffffffu, rw[kHLane - 1], 1);
@@ -455,14 +440,14 @@ __device__ __forceinline__ bool hcsr_seg_rows(const uint32_t* __restrict__ rp, i
       }
 #pragma unroll
       for (int i = 0; i < kHLane; ++i) {
-        const bool ok = COO ? rw[i] != 0xFFFFFFFFu : a + i >= lo && a + i < hi;
+        const bool ok = rw[i] != 0xFFFFFFFFu;
         if constexpr (MIX) p[i] = ok ? to_f32(vv[i]) * (float)ld_keep(xb + cc[i], pl) : 0.f;
         else p[i] = ok ? vv[i] * ld_keep(xb + cc[i], pl) : PT(0);
       }
     }
     // ---- marks of the rows that start inside the chunk
     uint32_t mb = 0;
-    if constexpr (COO) {
+    {
       // a row starts where it differs from the previous kept nonzero's
       uint32_t prev = __shfl_up_sync(0xffffffffu, rw[kHLane - 1], 1);
       if (lane == 0) prev = last_kept;
@@ -473,25 +458,6 @@ __device__ __forceinline__ bool hcsr_seg_rows(const uint32_t* __restrict__ rp, i
       }
       const uint32_t k31 = __shfl_sync(0xffffffffu, rw[kHLane - 1], 31);
       last_kept = k31 != 0xFFFFFFFFu ? k31 : last_kept;
-    } else {
-      mgrp[lane] = 0u;
-      __syncwarp();
-      for (;;) {
-        const int64_t pos = bp + (int64_t)s_c - c;
-        if (wb + lane < rb && pos >= 0 && pos < kHChunk && s_c < e_c) {
-          table[pos] = wb + lane;
-          atomicOr(mgrp + pos / kHLane, 1u << (pos % kHLane));
-        }
-        const uint32_t s31 = __shfl_sync(0xffffffffu, s_c, 31);
-        const bool exhausted = wb + 32 < rb && bp + (int64_t)s31 - c < kHChunk;
-        if (!exhausted) break;
-        wb += 32;
-        s_c = s_n;
-        e_c = e_n;
-        ldwin(wb + 32, s_n, e_n);
-      }
-      __syncwarp();
-      mb = mgrp[lane];
     }
     // ---- lane sums split at the marks; rows closed inside the lane are added now
     Ac sum, lead;
@@ -503,8 +469,7 @@ __device__ __forceinline__ bool hcsr_seg_rows(const uint32_t* __restrict__ rp, i
       if ((mb >> i) & 1u) {
         if (nf == 0) lead = sum;
         else hcsr_add(acc, rcur, acc_carry(sum));
-        if constexpr (COO) rcur = (int)rw[i];
-        else rcur = table[kHLane * lane + i];
+        rcur = (int)rw[i];
         ++nf;
         acc_zero(sum);
       }
@@ -656,9 +621,8 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
           continue;
         }
         if (klo == khi) continue;
-        if (hcsr_seg_rows<V, X, SA, MIX, VEC, true>(rp, h.bp, ra, rb, (int64_t)h.bp + klo, (int64_t)h.bp + khi, nz,
-                                                    col_idx, values, x + (int64_t)h.j * C, acc, table, mgrp, lane,
-                                                    pf, pl))
+        if (hcsr_coo_rows<V, X, SA, MIX, VEC>(rp, h.bp, ra, rb, (int64_t)h.bp + klo, (int64_t)h.bp + khi, nz, col_idx,
+                                              values, x + (int64_t)h.j * C, acc, lane, pf, pl))
           s_bad = 1;
       }
     }
