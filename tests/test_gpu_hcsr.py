@@ -148,6 +148,27 @@ def test_hcsr_coo_rows_out_of_order(how):
     assert np.array_equal(a, run(H, 1.0, x, 0.5, y0))
 
 
+def test_hcsr_large_coo_blocks_all_forms():
+    """COO blocks of thousands of nonzeros (p large: every block COO), which
+    the kernel streams by row range: fp64, fp32 and the mixed forms against
+    the oracle, and bitwise repeatable."""
+    m, n, Rst, Col, Val = W.powerlaw(300000, seed=13)
+    x, y0 = W.vector(n, 3), W.vector(m, 4)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.5, y0)
+    H = hcsr(m, n, Rst, Col, Val, torch.float64, R=4000, C=1 << 16, p=50.0)
+    cnt = np.diff(H.block_ptr.cpu().numpy())
+    assert (cnt >= 1024).sum() > 20  # the row-range path is taken
+    a = run(H, 1.0, x, 0.5, y0)
+    assert O.normwise_relerr(a, yref) < 1e-12
+    assert np.array_equal(a, run(H, 1.0, x, 0.5, y0))
+    H32 = hcsr(m, n, Rst, Col, Val.astype(np.float32), torch.float32, R=4000, C=1 << 16, p=50.0)
+    x32, y32 = x.astype(np.float32), y0.astype(np.float32)
+    assert O.normwise_relerr(run(H32, 1.0, x32, 0.5, y32), yref) < 1e-5
+    mixed = run(H32, 1.0, x32, 0.5, y32, mixed=True)
+    assert O.normwise_relerr(mixed, yref) < 1e-6
+    assert np.array_equal(mixed, run(H32, 1.0, x32, 0.5, y32, mixed=True))
+
+
 @pytest.mark.parametrize("dt", [np.float64, np.float32])
 def test_hcsr_unaligned_arrays(dt):
     """values / col_idx not 16-byte aligned (scalar loads) give the same
