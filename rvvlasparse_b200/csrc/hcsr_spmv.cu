@@ -45,6 +45,8 @@
 //     order (an integer atomicMin over a per-warp slot table elects the
 //     lowest pending lane of each row per round).
 // The next round's loads are issued before the current round is applied.
+// A COO row index at or beyond the block row's rows (malformed input; the
+// builder never writes one) is skipped rather than written out of range.
 // Per row, the sum is: row-range pieces of window 0 in block order, COO
 // products of window 0 in stream order, then window 1, ...; y = alpha*acc +
 // beta*y at the end (y is not read when beta == 0).  Shared memory is sized
@@ -667,6 +669,7 @@ hcsr_spmv_kernel(int64_t R, int64_t C, int64_t m, int64_t nz, int64_t b_n, const
             r.col = (uint32_t)ld_stream(col_idx + k, pf);
             r.v = ld_stream(values + k, pf);
             r.xoff = (int64_t)h.j * C;
+            r.ok = r.row < (uint32_t)rows;  // a row beyond the block row (malformed input) is skipped
           }
           ia = __shfl_sync(0xffffffffu, blk, 31);
         }

@@ -148,6 +148,34 @@ def test_hcsr_coo_rows_out_of_order(how):
     assert np.array_equal(a, run(H, 1.0, x, 0.5, y0))
 
 
+@pytest.mark.parametrize("p_", [50.0, 2.0])
+def test_hcsr_coo_row_beyond_block_row_is_skipped(p_):
+    """A hand-made HCSR whose COO nonzero names a row beyond its block row
+    (the reference would write out of range): that nonzero is left out and
+    every other row is right."""
+    m, n, Rst, Col, Val = W.powerlaw(50000, seed=14)
+    x, y0 = W.vector(n, 5), W.vector(m, 6)
+    yref = O.crs_spmv_ld(O.crs(m, n, Rst, Col, Val), 1.0, x, 0.5, y0)
+    H = hcsr(m, n, Rst, Col, Val, torch.float64, R=512, C=4096, p=p_)
+    h = H.to_host()
+    bp = h["block_ptr"].astype(np.int64)
+    ro = h["row_offset"].view(np.uint32)
+    rows = h["row_ptr"].view(np.uint32).copy()
+    cnt = np.diff(bp)
+    b = int(np.flatnonzero((cnt > 0) & ((ro[:-1] >> 30) != 1))[len(np.flatnonzero((cnt > 0) & ((ro[:-1] >> 30) != 1))) // 2])
+    off = int(ro[b] & 0x3FFFFFFF)
+    r_loc = int(rows[off])
+    rows[off] = 60000  # beyond the 512 rows of the block row
+    b_row, b_col = b // H.b_n, b % H.b_n
+    k = int(bp[b])
+    c_glob = b_col * H.C + int(h["col_idx"].view(np.uint16)[k])
+    expect = yref.copy()
+    expect[b_row * H.R + r_loc] -= h["values"][k] * x[c_glob]
+    H.row_ptr = dev(rows.view(np.int32))
+    a = run(H, 1.0, x, 0.5, y0)
+    assert O.normwise_relerr(a, expect) < 1e-12
+
+
 def test_hcsr_large_coo_blocks_all_forms():
     """COO blocks of thousands of nonzeros (p large: every block COO), which
     the kernel streams by row range: fp64, fp32 and the mixed forms against
