@@ -7,8 +7,9 @@ back with the table of all timings.  Candidates:
 
 * ``csr5``  sigma in {8, 16, 24, 32} (omega is fixed to a warp, 32);
 * ``sell``  C = 32 (a warp per slice) with sigma in {32, 256, 1024, 8192};
-* ``hcsr``  square blocks R = C in {512, 1024, 2000, 4000, 8192} and
-  R in {1000, 2000, 4000} with C = 65536, p = 2;
+* ``hcsr``  square blocks R = C in {512, 1024, 2000, 4000, 8192},
+  R in {1000, 2000, 4000} with C = 65536, and C = 65536 with R making the
+  block rows 2, 3 or 4 whole waves of two CTAs per SM, p = 2;
 * ``vhcc``  threads in {nnz/4096, nnz/2048, nnz/1024} (vectors of 32);
 * ``cvr``   ranges of {8192, 32768, 131072} nonzeros;
 * ``lav``   segment_len in {40000, n/4, n} (SIMD_Lanes 8, T 0.2).

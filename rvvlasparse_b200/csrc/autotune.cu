@@ -6,8 +6,9 @@
 // caller's CRS, one product is run untimed, then `iters` products are timed
 // with CUDA events on `stream` and the best time kept; the build is freed
 // before the next candidate.  Candidates per format:
-//   HCSR   square blocks R = C in {512, 1024, 2000, 4000, 8192} and
-//          R in {1000, 2000, 4000} with C = 65536, p = 2;
+//   HCSR   square blocks R = C in {512, 1024, 2000, 4000, 8192},
+//          R in {1000, 2000, 4000} with C = 65536, and C = 65536 with R
+//          making b_m 2, 3 or 4 waves of two CTAs per SM, p = 2;
 //   SELL   C = 32 (a warp per slice), sigma in {32, 256, 1024, 8192};
 //   CSR5   omega = 32, sigma in {8, 16, 24, 32};
 //   LAV    SIMD_Lanes 8, T 0.2, segment_len in {40000, n/4, n};
@@ -43,6 +44,15 @@ std::vector<rvvla_tune_params> candidates(int fmt, const rvvla_crs* A) {
       for (int64_t r : {1000, 2000, 4000}) {
         auto p = blank();
         p.R = r;
+        p.C = 65536;
+        out.push_back(p);
+      }
+      // block rows in whole waves: the kernel runs a CTA per block row, two
+      // per SM, so b_m a multiple of 2 x SMs leaves no partial last wave
+      for (int64_t waves : {2, 3, 4}) {
+        const int64_t slots = 2 * (int64_t)sm_count() * waves;
+        auto p = blank();
+        p.R = std::max<int64_t>(1, (A->m + slots - 1) / slots);
         p.C = 65536;
         out.push_back(p);
       }
