@@ -21,6 +21,7 @@ whole workload (weak scaling, no collective on the data path).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -338,6 +339,8 @@ def run_gpu(args):
     l0 = lib.rvvla_kernel_launch_count()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    gc.collect()
+    gc.disable()  # no collector pause of the launching thread inside the timed region
     t_start.record(stream)
     for s in range(args.steps):
         for c, (e0, e1) in zip(cases, ev[s]):
@@ -346,6 +349,7 @@ def run_gpu(args):
             e1.record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     launches = lib.rvvla_kernel_launch_count() - l0
     if world > 1:
         dist.barrier()
