@@ -68,3 +68,21 @@ def test_reference_arm_loads_no_cuda_library():
     assert all(c.split("_")[0] in ("crs", "hcsr", "sell", "lav", "cvr")
                for c in line["cpu_baseline"]["parts"]["reference_library"]["cases"])
     assert lines[-1] == "LOADED False False"
+
+
+def test_params_override_parses_and_is_recorded():
+    """--params "fmt:key=value,...;fmt2:..." becomes per-format convertParams
+    (ints stay ints, decimals become floats) and is recorded in the config."""
+    sys.path.insert(0, ROOT)
+    import argparse
+
+    import bench
+
+    p = bench.parse_params("hcsr:R=2000,C=65536;lav:T=0.2,segment_len=40000; ;csr5:sigma=24")
+    assert p == {"hcsr": {"R": 2000, "C": 65536}, "lav": {"T": 0.2, "segment_len": 40000}, "csr5": {"sigma": 24}}
+    assert isinstance(p["hcsr"]["R"], int) and isinstance(p["lav"]["T"], float)
+    assert bench.parse_params("") == {}
+    args = argparse.Namespace(workload="powerlaw", params="hcsr:R=100")
+    cfg = bench.config_for(args, 10, 20, ["hcsr_f64"], 1)
+    assert cfg["params"] == {"hcsr": {"R": 100}}
+    assert "params" not in bench.config_for(argparse.Namespace(workload="powerlaw", params=""), 10, 20, [], 1)
